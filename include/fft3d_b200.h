@@ -1,0 +1,118 @@
+/*
+ * fft3d_b200.h — C ABI of the B200 (sm_100a) FFT3D filtering core.
+ *
+ * This is the drop-in boundary for the per-plane engine of neo_fft3d:
+ * one fft3d_plane replaces one FFT3DEngine (reference src/fft3d_engine.h:22-741),
+ * which the plugin filter creates per processed plane (src/fft3d.hpp:186-198)
+ * and calls once per output frame (src/fft3d.hpp:241). Everything below takes
+ * plain pointers and sizes; no CUDA or torch types appear in the signatures
+ * (a CUDA stream is passed as void*).
+ *
+ * All functions return FFT3D_OK (0) or a negative FFT3D_E_* status; the
+ * message of the last failure on the calling thread is fft3d_last_error().
+ * Parameter errors carry the reference's own messages
+ * (src/fft3d_engine.h:105-126, src/fft3d.hpp:143-147).
+ *
+ * Threading: a plane handle is internally locked, so concurrent calls on one
+ * handle are serialised (like the reference's cache mutex). Distinct handles
+ * run concurrently; each owns one CUDA stream.
+ */
+#ifndef FFT3D_B200_H
+#define FFT3D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FFT3D_OK 0
+#define FFT3D_E_PARAM (-1)       /* invalid parameter (reference-compatible message) */
+#define FFT3D_E_CUDA (-2)        /* CUDA runtime or launch failure */
+#define FFT3D_E_UNSUPPORTED (-3) /* valid for the reference, not built here (see message) */
+#define FFT3D_E_NOMEM (-4)       /* device allocation failed */
+#define FFT3D_E_FRAME (-5)       /* a frame the call needs was not supplied */
+#define FFT3D_E_NOLIB (-6)       /* no CUDA device / driver */
+
+/* Filter parameters: the parameter surface of neo_fft3d (src/fft3d.hpp:29-73)
+ * with the reference's meanings. Defaults: fft3d_params_default()
+ * (src/fft3d.hpp:77-106). Field names follow EngineParams
+ * (src/fft3d_common.h:61-100). Booleans are ints. */
+typedef struct fft3d_params {
+  float sigma, beta;
+  int bw, bh, bt, ow, oh;
+  float kratio, sharpen, scutoff, svr, smin, smax;
+  int measure, interlaced, wintype;
+  int pframe, px, py, pshow;
+  float pcutoff, pfactor;
+  float sigma2, sigma3, sigma4;
+  float degrid, dehalo, hr, ht;
+  int l, t, r, b;
+  int opt, ncpu, mt;
+} fft3d_params;
+
+/* One plane of a clip, as the engine sees it (src/fft3d.hpp:186-192). */
+typedef struct fft3d_plane_desc {
+  int width, height;   /* plane size in pixels (already subsampled for chroma) */
+  int bits;            /* bits per sample: 8 (uint8), 9..16 (uint16), 32 (float) */
+  int is_chroma;       /* YUV chroma plane: integer samples are centred on 2^(bits-1) */
+  int ssw, ssh;        /* subsampling shifts applied to the crop l/r and t/b */
+  int num_frames;      /* clip length; frames near either end use bt = 1 */
+} fft3d_plane_desc;
+
+typedef struct fft3d_plane fft3d_plane;
+
+/* Reference defaults (src/fft3d.hpp:77-106): sigma 2, beta 1, bw=bh=32, bt=3,
+ * ow=oh=-1 (-> bw/3), kratio 2, sharpen 0, scutoff 0.3, svr 1, smin 4,
+ * smax 20, measure 1, wintype 0, pcutoff 0.1, pfactor 0, sigma2..4 = sigma,
+ * degrid 1, dehalo 0, hr 2, ht 50, ncpu 2. */
+void fft3d_params_default(fft3d_params* p);
+
+/* Create a plane engine on CUDA device `device`.
+ * Replaces FFT3DEngine::FFT3DEngine (src/fft3d_engine.h:87-408). */
+int fft3d_plane_create(const fft3d_params* p, const fft3d_plane_desc* d, int device, fft3d_plane** out);
+
+/* Filter output frame n of this plane from HOST memory.
+ * Replaces FFT3DEngine::GetFrame (src/fft3d_engine.h:452-734).
+ * src[2+d] is frame n+d for d in [-2, 2] (the reference's apply_in[] slots,
+ * src/fft3d_engine.h:634-644); only d in [-bt/2, (bt-1)/2] is read, and a slot
+ * may be NULL when that frame's spectrum is already cached on the device
+ * (query with fft3d_plane_cached). src_stride / dst_stride are in bytes.
+ * The whole plane is written to dst: the crop borders (l, t, r, b) are copied
+ * from src[2], as the plugin filter does (src/fft3d.hpp:292-352). */
+int fft3d_plane_filter(fft3d_plane* h, int n, const void* const src[5], const int src_stride[5], void* dst,
+                       int dst_stride);
+
+/* Same as fft3d_plane_filter, but src/dst are DEVICE pointers and the work is
+ * queued on `stream` (a cudaStream_t; NULL = the handle's own stream) without
+ * a host synchronisation. */
+int fft3d_plane_filter_device(fft3d_plane* h, int n, const void* const src[5], const int src_stride[5], void* dst,
+                              int dst_stride, void* stream);
+
+/* 1 if the spectrum of frame n is held in the device spectrum cache. */
+int fft3d_plane_cached(fft3d_plane* h, int n);
+
+/* Copy the forward spectrum of frame n (which must be cached) to host memory
+ * as blocks x bh x (bw/2+1) complex floats (interleaved re, im; no padding). */
+int fft3d_plane_spectrum(fft3d_plane* h, int n, float* out);
+
+/* Geometry: out[0..7] = nox, noy, cover width, cover height, bw/2+1, blocks,
+ * ow, oh (after the ow/oh = bw/3 default is applied). */
+int fft3d_plane_geometry(fft3d_plane* h, int out[8]);
+
+/* Drop all cached spectra and reset the Kalman state to its initial values. */
+int fft3d_plane_reset(fft3d_plane* h);
+
+void fft3d_plane_destroy(fft3d_plane* h);
+
+/* Message of the last failure on this thread ("" if none). */
+const char* fft3d_last_error(void);
+
+/* Number of kernels this library has launched in this process (all handles). */
+uint64_t fft3d_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FFT3D_B200_H */
