@@ -101,6 +101,13 @@ int fft3d_plane_spectrum(fft3d_plane* h, int n, float* out);
  * ow, oh (after the ow/oh = bw/3 default is applied). */
 int fft3d_plane_geometry(fft3d_plane* h, int out[8]);
 
+/* Estimate the noise pattern (pfactor != 0) from one frame in HOST memory, as
+ * the reference does from frame pframe on its first GetFrame
+ * (src/fft3d_engine.h:485-504, src/helper.cpp:46-132): block (px, py), or the
+ * quietest block when px = py = 0. Required before the first filter call of a
+ * pattern-mode plane; a no-op otherwise. */
+int fft3d_plane_set_pattern_frame(fft3d_plane* h, const void* src, int src_stride);
+
 /* Drop all cached spectra and reset the Kalman state to its initial values. */
 int fft3d_plane_reset(fft3d_plane* h);
 

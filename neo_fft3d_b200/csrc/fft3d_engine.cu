@@ -1,0 +1,642 @@
+// Per-plane engine and C ABI (include/fft3d_b200.h) of the FFT3D filtering
+// core. One fft3d_plane is the B200 counterpart of one FFT3DEngine
+// (reference src/fft3d_engine.h:22-741): it owns the plane's tables, a device
+// ring of per-frame spectra (the reference's LRU cache, src/cache.hpp:18-78),
+// the Kalman state and one CUDA stream.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "fft3d_b200.h"
+#include "fft3d_kernels.cuh"
+
+using fft3d::Geom;
+
+namespace {
+
+thread_local std::string g_err;
+std::atomic<uint64_t> g_launches{0};
+std::mutex g_dev_lock;
+std::vector<int> g_tw_ready;  // devices whose twiddle tables are uploaded
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(FFT3D_E_CUDA, std::string("neo_fft3d: CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call, what)                            \
+  do {                                            \
+    cudaError_t e_ = (call);                      \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+struct Slot {
+  float2* spec = nullptr;
+  int frame = -1;
+  uint64_t stamp = 0;
+};
+
+}  // namespace
+
+struct fft3d_plane {
+  std::mutex mu;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  fft3d_params ep{};
+  fft3d_plane_desc d{};
+  int bytes = 1;
+  Geom g{};
+  int l = 0, t = 0;  // crop origin (plane units)
+  float norm = 0, sigma2n_2d = 0, smin2n = 0, smax2n = 0, ht2n = 0;
+  bool pattern = false, pattern_set = false, pattern3d_init = false;
+  std::vector<float> h_pattern2d, h_pwin, h_grid;  // h_grid: bh*nh complex
+  // device tables (one allocation)
+  void* d_tables = nullptr;
+  fft3d::Tables tab{};
+  const float* d_wan_x = nullptr;
+  const float* d_wan_y = nullptr;
+  float* d_pattern2d = nullptr;
+  float* d_pattern3d = nullptr;
+  std::vector<Slot> slots;
+  uint64_t clock = 0;
+  float* d_tdom = nullptr;
+  float2* d_last = nullptr;
+  float* d_cov = nullptr;
+  float* d_covp = nullptr;
+  void* d_in = nullptr;   // staging of host frames (whole plane)
+  size_t in_pitch = 0;
+  void* d_out = nullptr;  // staging of the host output (whole plane)
+  size_t out_pitch = 0;
+  size_t spec_elems() const { return (size_t)g.nblocks * g.bh * g.nh; }
+};
+
+namespace {
+
+// ---------------------------------------------------------------- tables
+// Same formulas as the reference's constructor (src/fft3d_engine.h:204-375),
+// computed in float with the double exp/sqrt the reference's C++ calls.
+
+void windows(const fft3d_params& ep, int o, std::vector<float>& anl, std::vector<float>& anr,
+             std::vector<float>& snl, std::vector<float>& snr) {
+  const float pi = 3.1415926535897932384626433832795f;
+  anl.assign(o, 1.f); anr.assign(o, 1.f); snl.assign(o, 1.f); snr.assign(o, 1.f);
+  for (int i = 0; i < o; i++) {
+    float cl = cosf(pi * (i - o + 0.5f) / (o * 2)), cr = cosf(pi * (i + 0.5f) / (o * 2));
+    if (ep.wintype == 0) {
+      anl[i] = cl; anr[i] = cr; snl[i] = cl; snr[i] = cr;
+    } else if (ep.wintype == 1) {
+      anl[i] = (float)std::sqrt((double)cl); anr[i] = (float)std::sqrt((double)cr);
+      snl[i] = anl[i] * anl[i] * anl[i]; snr[i] = anr[i] * anr[i] * anr[i];
+    } else {
+      snl[i] = cl * cl; snr[i] = cr * cr;
+    }
+  }
+}
+
+std::vector<float> full_window(int b, int o, const std::vector<float>& l, const std::vector<float>& r) {
+  std::vector<float> w(b, 1.f);
+  for (int i = 0; i < o; i++) {
+    w[i] = l[i];
+    w[b - o + i] = r[i];
+  }
+  return w;
+}
+
+// gridsample: the spectrum of one windowed block of maximum-value samples
+// (src/fft3d_engine.h:380-404). The block is separable, so its 2D DFT is the
+// outer product of two 1D DFTs; evaluated in double, rounded to float.
+void gridsample(const std::vector<float>& wx, const std::vector<float>& wy, double maxv, int bw, int bh,
+                std::vector<float>& out) {
+  int nh = bw / 2 + 1;
+  std::vector<double> xr(nh), xi(nh), yr(bh), yi(bh);
+  for (int k = 0; k < nh; k++) {
+    double sr = 0, si = 0;
+    for (int x = 0; x < bw; x++) {
+      double a = -2.0 * M_PI * (double)((long)k * x % bw) / bw;
+      sr += wx[x] * std::cos(a);
+      si += wx[x] * std::sin(a);
+    }
+    xr[k] = sr; xi[k] = si;
+  }
+  for (int h = 0; h < bh; h++) {
+    double sr = 0, si = 0;
+    for (int y = 0; y < bh; y++) {
+      double a = -2.0 * M_PI * (double)((long)h * y % bh) / bh;
+      sr += wy[y] * std::cos(a);
+      si += wy[y] * std::sin(a);
+    }
+    yr[h] = sr; yi[h] = si;
+  }
+  out.assign((size_t)bh * nh * 2, 0.f);
+  for (int h = 0; h < bh; h++)
+    for (int k = 0; k < nh; k++) {
+      out[2 * (h * nh + k)] = (float)(maxv * (yr[h] * xr[k] - yi[h] * xi[k]));
+      out[2 * (h * nh + k) + 1] = (float)(maxv * (yr[h] * xi[k] + yi[h] * xr[k]));
+    }
+}
+
+// FindPatternBlock / SetPattern (src/helper.cpp:46-132) on a host copy of
+// the spectrum of frame pframe.
+void estimate_pattern(fft3d_plane* P, const std::vector<float2>& spec) {
+  const int nh = P->g.nh, nb = P->g.bh * nh;
+  const float* gs = P->h_grid.data();
+  auto power = [&](const float2* s, int i, float gcur) {
+    float c0 = s[i].x - gcur * gs[2 * i], c1 = s[i].y - gcur * gs[2 * i + 1];
+    return c0 * c0 + c1 * c1;
+  };
+  if (P->ep.px == 0 && P->ep.py == 0) {
+    float best = 1e15f;
+    for (int by = 2; by < P->g.noy - 2; by++)
+      for (int bx = 2; bx < P->g.nox - 2; bx++) {
+        const float2* s = spec.data() + ((size_t)by * P->g.nox + bx) * nb;
+        float gcur = P->ep.degrid * s[0].x / gs[0];
+        float acc = 0;
+        for (int i = 0; i < nb; i++) acc += power(s, i, gcur) * P->h_pwin[i];
+        if (acc < best) { P->ep.px = bx; P->ep.py = by; best = acc; }
+      }
+  }
+  const float2* s = spec.data() + ((size_t)P->ep.py * P->g.nox + P->ep.px) * nb;
+  float gcur = P->ep.degrid * s[0].x / gs[0];
+  for (int i = 0; i < nb; i++) P->h_pattern2d[i] = power(s, i, gcur) * P->h_pwin[i];
+}
+
+int ensure_twiddles(int dev) {
+  std::lock_guard<std::mutex> lk(g_dev_lock);
+  if (std::find(g_tw_ready.begin(), g_tw_ready.end(), dev) != g_tw_ready.end()) return FFT3D_OK;
+  CK(fft3d::upload_twiddles(), "twiddle upload");
+  g_tw_ready.push_back(dev);
+  return FFT3D_OK;
+}
+
+void free_plane(fft3d_plane* P) {
+  if (!P) return;
+  cudaSetDevice(P->device);
+  if (P->stream) cudaStreamSynchronize(P->stream);
+  for (auto& s : P->slots) cudaFree(s.spec);
+  cudaFree(P->d_tables);
+  cudaFree(P->d_tdom);
+  cudaFree(P->d_last);
+  cudaFree(P->d_cov);
+  cudaFree(P->d_covp);
+  cudaFree(P->d_in);
+  cudaFree(P->d_out);
+  if (P->stream) cudaStreamDestroy(P->stream);
+  delete P;
+}
+
+int upload_pattern(fft3d_plane* P, float* dptr, const std::vector<float>& v) {
+  CK(cudaMemcpyAsync(dptr, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice, P->stream), "pattern upload");
+  return FFT3D_OK;
+}
+
+Slot* find_slot(fft3d_plane* P, int frame) {
+  for (auto& s : P->slots)
+    if (s.frame == frame) return &s;
+  return nullptr;
+}
+
+// least recently used slot whose frame is not in [lo, hi]
+Slot* evict_slot(fft3d_plane* P, int lo, int hi) {
+  Slot* best = nullptr;
+  for (auto& s : P->slots) {
+    if (s.frame >= lo && s.frame <= hi) continue;
+    if (!best || s.stamp < best->stamp) best = &s;
+  }
+  return best;
+}
+
+int launch_forward(fft3d_plane* P, const void* plane, long long stride, float2* spec, cudaStream_t st) {
+  fft3d::ForwardArgs a;
+  a.g = P->g;
+  a.src = static_cast<const char*>(plane) + (long long)P->t * stride + (long long)P->l * P->bytes;
+  a.src_stride = stride;
+  a.base = (P->bytes != 4 && P->d.is_chroma) ? (float)(1 << (P->d.bits - 1)) : 0.f;
+  a.wan_x = P->d_wan_x;
+  a.wan_y = P->d_wan_y;
+  a.spec = spec;
+  CK(fft3d::launch_forward(a, P->bytes, st), "forward kernel");
+  g_launches++;
+  return FFT3D_OK;
+}
+
+// The spectrum of frame m in a ring slot, computing it from `plane` if needed.
+int spectrum_slot(fft3d_plane* P, int m, int lo, int hi, const void* plane, int stride, bool host, cudaStream_t st,
+                  Slot** out) {
+  Slot* s = find_slot(P, m);
+  if (!s) {
+    if (!plane) return fail(FFT3D_E_FRAME, "neo_fft3d: frame " + std::to_string(m) + " is needed but was not supplied");
+    s = evict_slot(P, lo, hi);
+    if (!s) return fail(FFT3D_E_PARAM, "neo_fft3d: spectrum ring too small");
+    s->frame = -1;
+    const void* src = plane;
+    long long sstride = stride;
+    if (host) {
+      CK(cudaMemcpy2DAsync(P->d_in, P->in_pitch, plane, stride, (size_t)P->d.width * P->bytes, P->d.height,
+                           cudaMemcpyHostToDevice, st), "frame upload");
+      src = P->d_in;
+      sstride = (long long)P->in_pitch;
+    }
+    int rc = launch_forward(P, src, sstride, s->spec, st);
+    if (rc) return rc;
+    s->frame = m;
+  }
+  s->stamp = ++P->clock;
+  *out = s;
+  return FFT3D_OK;
+}
+
+int copy_plane(fft3d_plane* P, void* dst, int dstride, const void* src, int sstride, cudaMemcpyKind kind,
+               cudaStream_t st) {
+  CK(cudaMemcpy2DAsync(dst, dstride, src, sstride, (size_t)P->d.width * P->bytes, P->d.height, kind, st),
+     "plane copy");
+  return FFT3D_OK;
+}
+
+int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride[5], void* dst, int dst_stride,
+               bool host, cudaStream_t st) {
+  const fft3d_params& ep = P->ep;
+  const int bt = ep.bt;
+  int btcur = bt;  // src/fft3d_engine.h:579-582
+  if ((bt / 2 > n) || (bt - 1) / 2 > (P->d.num_frames - 1 - n)) btcur = 1;
+  const void* cur = src ? src[2] : nullptr;
+  if (bt == 0 && n == 0) {  // Kalman: frame 0 is returned unprocessed (:681-687)
+    if (!cur) return fail(FFT3D_E_FRAME, "neo_fft3d: frame 0 was not supplied");
+    int rc = copy_plane(P, dst, dst_stride, cur, stride[2], host ? cudaMemcpyHostToHost : cudaMemcpyDeviceToDevice, st);
+    if (rc) return rc;
+    if (host) CK(cudaStreamSynchronize(st), "synchronize");
+    return FFT3D_OK;
+  }
+  if (P->pattern && !P->pattern_set)
+    return fail(FFT3D_E_PARAM, "neo_fft3d: noise pattern not estimated yet (fft3d_plane_set_pattern_frame)");
+  const int from = bt > 0 && btcur > 1 ? -btcur / 2 : 0;
+  const int to = bt > 0 && btcur > 1 ? (btcur - 1) / 2 : 0;
+  fft3d::InverseArgs ia{};
+  for (int d = from; d <= to; d++) {
+    Slot* s = nullptr;
+    int rc = spectrum_slot(P, n + d, n + from, n + to, src ? src[2 + d] : nullptr, stride ? stride[2 + d] : 0, host,
+                           st, &s);
+    if (rc) return rc;
+    ia.in[2 + d] = s->spec;
+  }
+  if (bt > 0 && btcur > 1 && P->pattern && !P->pattern3d_init) {  // :625-630
+    std::vector<float> p3(P->h_pattern2d.size());
+    for (size_t i = 0; i < p3.size(); i++) p3[i] = P->h_pattern2d[i] * (float)btcur;
+    int rc = upload_pattern(P, P->d_pattern3d, p3);
+    if (rc) return rc;
+    P->pattern3d_init = true;
+  }
+  const int mode = bt > 0 ? btcur : bt;
+  ia.g = P->g;
+  ia.t = P->tab;
+  fft3d::FilterConsts& c = ia.c;
+  c.sigma2n = btcur * ep.sigma * ep.sigma / P->norm;  // :589
+  c.sigma2n_2d = P->sigma2n_2d;
+  c.lowlimit = (ep.beta - 1) / ep.beta;
+  c.degrid = ep.degrid;
+  c.sharpen = ep.sharpen;
+  c.dehalo = ep.dehalo;
+  c.smin2n = P->smin2n;
+  c.smax2n = P->smax2n;
+  c.ht2n = P->ht2n;
+  c.kratio2 = ep.kratio * ep.kratio;
+  c.pattern = P->pattern ? 1 : 0;
+  c.use_sharpen = ep.sharpen != 0;
+  c.use_dehalo = ep.dehalo != 0;
+  c.fuse_sharpen = (mode == 1 && !P->pattern) ? 1 : 0;
+  c.do_sharpen = ((ep.sharpen != 0 || ep.dehalo != 0) && (mode != 1 || P->pattern)) ? 1 : 0;
+  ia.kal_last = P->d_last;
+  ia.kal_covar = P->d_cov;
+  ia.kal_covarp = P->d_covp;
+  ia.tdom = P->d_tdom;
+  CK(fft3d::launch_filter_inverse(ia, mode, st), "filter/inverse kernel");
+  g_launches++;
+  // output: the crop borders come from the source frame (src/fft3d.hpp:292-352)
+  const bool crop = ep.l > 0 || ep.t > 0 || ep.r > 0 || ep.b > 0;
+  void* odst = dst;
+  long long ostride = dst_stride;
+  if (host) {
+    odst = P->d_out;
+    ostride = (long long)P->out_pitch;
+    if (crop) {
+      if (!cur) return fail(FFT3D_E_FRAME, "neo_fft3d: the current frame is needed for the crop borders");
+      for (int y = 0; y < P->d.height; y++)
+        std::memcpy(static_cast<char*>(dst) + (size_t)y * dst_stride, static_cast<const char*>(cur) + (size_t)y * stride[2],
+                    (size_t)P->d.width * P->bytes);
+    }
+  } else if (crop) {
+    if (!cur) return fail(FFT3D_E_FRAME, "neo_fft3d: the current frame is needed for the crop borders");
+    int rc = copy_plane(P, dst, dst_stride, cur, stride[2], cudaMemcpyDeviceToDevice, st);
+    if (rc) return rc;
+  }
+  fft3d::OlaArgs oa;
+  oa.g = P->g;
+  oa.t = P->tab;
+  oa.tdom = P->d_tdom;
+  oa.dst = static_cast<char*>(odst) + (long long)P->t * ostride + (long long)P->l * P->bytes;
+  oa.dst_stride = ostride;
+  oa.norm = P->norm;
+  const bool ints = P->bytes != 4;
+  oa.rounder = ints ? 0.5f : 0.f;
+  oa.base = (ints && P->d.is_chroma) ? (float)(1 << (P->d.bits - 1)) : 0.f;
+  oa.maxval = P->bytes == 1 ? 255 : (1 << P->d.bits) - 1;
+  CK(fft3d::launch_overlap_add(oa, P->bytes, st), "overlap-add kernel");
+  g_launches++;
+  if (host) {
+    char* hdst = static_cast<char*>(dst) + (size_t)P->t * dst_stride + (size_t)P->l * P->bytes;
+    const char* ddst = static_cast<const char*>(P->d_out) + P->t * P->out_pitch + (size_t)P->l * P->bytes;
+    CK(cudaMemcpy2DAsync(hdst, dst_stride, ddst, P->out_pitch, (size_t)P->g.W * P->bytes, P->g.H,
+                         cudaMemcpyDeviceToHost, st), "result download");
+    CK(cudaStreamSynchronize(st), "synchronize");
+  }
+  return FFT3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void fft3d_params_default(fft3d_params* p) {
+  // src/fft3d.hpp:77-106
+  std::memset(p, 0, sizeof(*p));
+  p->sigma = 2.0f; p->beta = 1.0f;
+  p->bw = 32; p->bh = 32; p->bt = 3; p->ow = -1; p->oh = -1;
+  p->kratio = 2.0f; p->sharpen = 0.0f; p->scutoff = 0.3f; p->svr = 1.0f; p->smin = 4.0f; p->smax = 20.0f;
+  p->measure = 1; p->interlaced = 0; p->wintype = 0;
+  p->pframe = 0; p->px = 0; p->py = 0; p->pshow = 0;
+  p->pcutoff = 0.1f; p->pfactor = 0.0f;
+  p->sigma2 = p->sigma3 = p->sigma4 = 2.0f;
+  p->degrid = 1.0f; p->dehalo = 0.0f; p->hr = 2.0f; p->ht = 50.0f;
+  p->opt = 0; p->ncpu = 2; p->mt = 0;
+}
+
+const char* fft3d_last_error(void) { return g_err.c_str(); }
+
+uint64_t fft3d_kernel_launches(void) { return g_launches.load(); }
+
+int fft3d_plane_create(const fft3d_params* p, const fft3d_plane_desc* d, int device, fft3d_plane** out) {
+  if (!p || !d || !out) return fail(FFT3D_E_PARAM, "neo_fft3d: null argument");
+  *out = nullptr;
+  auto* P = new fft3d_plane();
+  P->ep = *p;
+  P->d = *d;
+  P->device = device;
+  fft3d_params& ep = P->ep;
+  if (d->bits < 8 || (d->bits > 16 && d->bits != 32)) { delete P; return fail(FFT3D_E_PARAM, "neo_fft3d: unsupported bit depth"); }
+  P->bytes = d->bits <= 8 ? 1 : (d->bits <= 16 ? 2 : 4);
+  // bit-depth scaling, src/fft3d_engine.h:91-103
+  float factor = P->bytes == 1 ? 1.0f : (P->bytes == 2 ? float(1 << (d->bits - 8)) : 1 / 255.0f);
+  ep.sigma *= factor; ep.sigma2 *= factor; ep.sigma3 *= factor; ep.sigma4 *= factor;
+  ep.smin *= factor; ep.smax *= factor;
+  // reference checks and defaults, src/fft3d_engine.h:105-126
+  if (ep.ow * 2 > ep.bw) { delete P; return fail(FFT3D_E_PARAM, "ow must be less than bw / 2"); }
+  if (ep.oh * 2 > ep.bh) { delete P; return fail(FFT3D_E_PARAM, "oh must be less than bh / 2"); }
+  if (ep.ow < 0) ep.ow = ep.bw / 3;
+  if (ep.oh < 0) ep.oh = ep.bh / 3;
+  if (ep.bt < -1 || ep.bt > 5) { delete P; return fail(FFT3D_E_PARAM, "bt must be -1 (Sharpen), 0 (Kalman), 1..5 (Wiener)"); }
+  if (ep.beta < 1) { delete P; return fail(FFT3D_E_PARAM, "beta must be not less 1.0"); }
+  if (!fft3d::block_size_supported(ep.bw, ep.bh)) {
+    delete P;
+    return fail(FFT3D_E_UNSUPPORTED, "neo_fft3d: block size " + std::to_string(ep.bw) + "x" + std::to_string(ep.bh) +
+                                         " is not built into this library (bw, bh in 8,12,16,24,32,48)");
+  }
+  if (ep.pshow) { delete P; return fail(FFT3D_E_UNSUPPORTED, "neo_fft3d: pshow is not supported by the GPU engine"); }
+  // crop in plane units, src/buffer.cpp:564-570
+  P->l = d->is_chroma ? (ep.l >> d->ssw) : ep.l;
+  int r = d->is_chroma ? (ep.r >> d->ssw) : ep.r;
+  P->t = d->is_chroma ? (ep.t >> d->ssh) : ep.t;
+  int b = d->is_chroma ? (ep.b >> d->ssh) : ep.b;
+  Geom& g = P->g;
+  g.W = d->width - P->l - r;
+  g.H = d->height - P->t - b;
+  if (g.W <= 0) { delete P; return fail(FFT3D_E_PARAM, "Width cannot be cropped to zero or below"); }
+  if (g.H <= 0) { delete P; return fail(FFT3D_E_PARAM, "Height cannot be cropped to zero or below"); }
+  if (ep.interlaced && (g.H & 1)) { delete P; return fail(FFT3D_E_UNSUPPORTED, "neo_fft3d: interlaced planes need an even height"); }
+  g.bw = ep.bw; g.bh = ep.bh; g.ow = ep.ow; g.oh = ep.oh;
+  g.sx = ep.bw - ep.ow; g.sy = ep.bh - ep.oh;
+  g.nox = (g.W - ep.ow + (ep.bw - ep.ow - 1)) / (ep.bw - ep.ow) + 2;  // :115-121
+  g.noy = (g.H - ep.oh + (ep.bh - ep.oh - 1)) / (ep.bh - ep.oh) + 2;
+  g.nblocks = g.nox * g.noy;
+  g.nh = ep.bw / 2 + 1;
+  g.interlaced = ep.interlaced ? 1 : 0;
+  // tables
+  std::vector<float> axl, axr, sxl, sxr, ayl, ayr, syl, syr;
+  windows(ep, ep.ow, axl, axr, sxl, sxr);
+  windows(ep, ep.oh, ayl, ayr, syl, syr);
+  std::vector<float> wx = full_window(ep.bw, ep.ow, axl, axr), wy = full_window(ep.bh, ep.oh, ayl, ayr);
+  const int bh = ep.bh, bw = ep.bw, nh = g.nh, nb = bh * nh;
+  std::vector<float> wsharpen(nb), wdehalo(nb);
+  float wmax = 0;
+  for (int j = 0; j < bh; j++) {  // :285-327
+    int dj = j >= bh / 2 ? bh - j : j;
+    float d2v = float(dj * dj) * (ep.svr * ep.svr) / ((bh / 2) * (bh / 2));
+    for (int i = 0; i < nh; i++) {
+      float d2 = d2v + float(i * i) / ((bw / 2) * (bw / 2));
+      wsharpen[j * nh + i] = (float)(1 - std::exp((double)(-d2 / (2 * ep.scutoff * ep.scutoff))));
+      float dh = (float)(std::exp((double)(-0.7f * d2 * ep.hr * ep.hr)) - std::exp((double)(-d2 * ep.hr * ep.hr)));
+      wdehalo[j * nh + i] = dh;
+      if (dh > wmax) wmax = dh;
+    }
+  }
+  for (auto& v : wdehalo) v /= wmax;
+  P->norm = 1.0f / (ep.bw * ep.bh);  // :329-336
+  P->sigma2n_2d = ep.sigma * ep.sigma / P->norm;
+  P->smin2n = ep.smin * ep.smin / P->norm;
+  P->smax2n = ep.smax * ep.smax / P->norm;
+  P->ht2n = ep.ht * ep.ht / P->norm;
+  P->h_pwin.assign(nb, 0.f);  // :346-361
+  for (int j = 0; j < bh; j++) {
+    int dj = std::min(j, bh - j);
+    float fh = dj * 2.0f / bh, fh2 = fh * fh;
+    for (int i = 0; i < nh; i++) {
+      float fw2 = (i * 2.0f / bw) * (i * 2.0f / bw);
+      P->h_pwin[j * nh + i] = (fh2 + fw2) / (fh2 + fw2 + ep.pcutoff * ep.pcutoff);
+    }
+  }
+  P->h_pattern2d.assign(nb, 0.f);
+  if ((ep.sigma2 != ep.sigma || ep.sigma3 != ep.sigma || ep.sigma4 != ep.sigma) && ep.pfactor == 0) {
+    // SigmasToPattern, src/helper.cpp:14-43; src/fft3d_engine.h:366-371
+    float ft2 = (float)(std::sqrt((double)0.5f) / 2), ft3 = (float)(std::sqrt((double)0.5f) / 4);
+    for (int h = 0; h < bh; h++)
+      for (int w = 0; w < nh; w++) {
+        float fy = (bh - 2.0f * std::abs(h - bh / 2)) / bh;
+        float fx = (w * 1.0f) / nh;
+        float f = (float)std::sqrt((double)((fx * fx + fy * fy) * 0.5f));
+        float s;
+        if (f < ft3) s = ep.sigma4 + (ep.sigma3 - ep.sigma4) * f / ft3;
+        else if (f < ft2) s = ep.sigma3 + (ep.sigma2 - ep.sigma3) * (f - ft3) / (ft2 - ft3);
+        else s = ep.sigma + (ep.sigma2 - ep.sigma) * (1 - f) / (1 - ft2);
+        P->h_pattern2d[h * nh + w] = s * s / P->norm;
+      }
+    P->pattern_set = true;
+    ep.pfactor = 1;
+  }
+  P->pattern = ep.pfactor != 0;
+  double maxv = P->bytes == 1 ? 255.0 : (P->bytes == 2 ? (double)((1 << d->bits) - 1) : 1.0);
+  gridsample(wx, wy, maxv, bw, bh, P->h_grid);
+
+  // device resources
+  int rc = FFT3D_OK;
+  auto bail = [&](int code) { free_plane(P); return code; };
+  {
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) { rc = cuda_fail(e, "cudaSetDevice"); return bail(rc == FFT3D_E_CUDA ? FFT3D_E_NOLIB : rc); }
+  }
+  if ((rc = ensure_twiddles(device))) return bail(rc);
+  {
+    cudaError_t e = cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "stream create"));
+  }
+  // one table allocation: wan_x, wan_y, wsyn_xl/xr, wsyn_yl/yr, grid, wsharpen, wdehalo, pattern2d, pattern3d
+  std::vector<float> blob;
+  auto put = [&](const std::vector<float>& v) {
+    size_t off = blob.size();
+    blob.insert(blob.end(), v.begin(), v.end());
+    while (blob.size() % 4) blob.push_back(0.f);
+    return off;
+  };
+  auto one = [](std::vector<float> v) { if (v.empty()) v.push_back(1.f); return v; };
+  size_t o_wx = put(wx), o_wy = put(wy), o_sxl = put(one(sxl)), o_sxr = put(one(sxr)), o_syl = put(one(syl)),
+         o_syr = put(one(syr)), o_grid = put(P->h_grid), o_wsh = put(wsharpen), o_wdh = put(wdehalo),
+         o_p2 = put(P->h_pattern2d), o_p3 = put(std::vector<float>(nb, 0.f));
+  {
+    cudaError_t e = cudaMalloc(&P->d_tables, blob.size() * sizeof(float));
+    if (e != cudaSuccess) return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (tables)"));
+    e = cudaMemcpy(P->d_tables, blob.data(), blob.size() * sizeof(float), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "table upload"));
+  }
+  float* T = static_cast<float*>(P->d_tables);
+  P->d_wan_x = T + o_wx;
+  P->d_wan_y = T + o_wy;
+  P->tab.wan_x = T + o_wx;
+  P->tab.wan_y = T + o_wy;
+  P->tab.wsyn_xl = T + o_sxl;
+  P->tab.wsyn_xr = T + o_sxr;
+  P->tab.wsyn_yl = T + o_syl;
+  P->tab.wsyn_yr = T + o_syr;
+  P->tab.grid = reinterpret_cast<const float2*>(T + o_grid);
+  P->tab.wsharpen = T + o_wsh;
+  P->tab.wdehalo = T + o_wdh;
+  P->d_pattern2d = T + o_p2;
+  P->d_pattern3d = T + o_p3;
+  P->tab.pattern2d = P->d_pattern2d;
+  P->tab.pattern3d = P->d_pattern3d;
+  // spectrum ring: bt frames for the window plus slack for look-ahead
+  int nslots = (ep.bt > 1 ? ep.bt : 1) + 2;
+  P->slots.resize(nslots);
+  for (auto& s : P->slots) {
+    if (cudaMalloc(&s.spec, P->spec_elems() * sizeof(float2)) != cudaSuccess)
+      return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (spectrum ring)"));
+  }
+  if (cudaMalloc(&P->d_tdom, (size_t)g.nblocks * bh * bw * sizeof(float)) != cudaSuccess)
+    return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (time-domain blocks)"));
+  if (ep.bt == 0) {  // Kalman state, :339-344
+    if (cudaMalloc(&P->d_last, P->spec_elems() * sizeof(float2)) != cudaSuccess ||
+        cudaMalloc(&P->d_cov, P->spec_elems() * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&P->d_covp, P->spec_elems() * sizeof(float)) != cudaSuccess)
+      return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (Kalman state)"));
+  }
+  if (cudaMallocPitch(&P->d_in, &P->in_pitch, (size_t)d->width * P->bytes, d->height) != cudaSuccess ||
+      cudaMallocPitch(&P->d_out, &P->out_pitch, (size_t)d->width * P->bytes, d->height) != cudaSuccess)
+    return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (staging)"));
+  *out = P;
+  if ((rc = fft3d_plane_reset(P))) { *out = nullptr; return bail(rc); }
+  return FFT3D_OK;
+}
+
+int fft3d_plane_reset(fft3d_plane* P) {
+  if (!P) return fail(FFT3D_E_PARAM, "neo_fft3d: null handle");
+  std::lock_guard<std::mutex> lk(P->mu);
+  CK(cudaSetDevice(P->device), "cudaSetDevice");
+  for (auto& s : P->slots) { s.frame = -1; s.stamp = 0; }
+  if (P->ep.bt == 0) {
+    const size_t n = P->spec_elems();
+    std::vector<float> init(n, P->sigma2n_2d);
+    CK(cudaMemsetAsync(P->d_last, 0, n * sizeof(float2), P->stream), "Kalman reset");
+    CK(cudaMemcpyAsync(P->d_cov, init.data(), n * sizeof(float), cudaMemcpyHostToDevice, P->stream), "Kalman reset");
+    CK(cudaMemcpyAsync(P->d_covp, init.data(), n * sizeof(float), cudaMemcpyHostToDevice, P->stream), "Kalman reset");
+    CK(cudaStreamSynchronize(P->stream), "Kalman reset");
+  }
+  return FFT3D_OK;
+}
+
+void fft3d_plane_destroy(fft3d_plane* P) { free_plane(P); }
+
+int fft3d_plane_filter(fft3d_plane* P, int n, const void* const src[5], const int src_stride[5], void* dst,
+                       int dst_stride) {
+  if (!P || !dst) return fail(FFT3D_E_PARAM, "neo_fft3d: null argument");
+  std::lock_guard<std::mutex> lk(P->mu);
+  CK(cudaSetDevice(P->device), "cudaSetDevice");
+  return run_filter(P, n, src, src_stride, dst, dst_stride, true, P->stream);
+}
+
+int fft3d_plane_filter_device(fft3d_plane* P, int n, const void* const src[5], const int src_stride[5], void* dst,
+                              int dst_stride, void* stream) {
+  if (!P || !dst) return fail(FFT3D_E_PARAM, "neo_fft3d: null argument");
+  std::lock_guard<std::mutex> lk(P->mu);
+  CK(cudaSetDevice(P->device), "cudaSetDevice");
+  return run_filter(P, n, src, src_stride, dst, dst_stride, false, stream ? (cudaStream_t)stream : P->stream);
+}
+
+int fft3d_plane_cached(fft3d_plane* P, int n) {
+  if (!P) return 0;
+  std::lock_guard<std::mutex> lk(P->mu);
+  return find_slot(P, n) ? 1 : 0;
+}
+
+int fft3d_plane_spectrum(fft3d_plane* P, int n, float* out) {
+  if (!P || !out) return fail(FFT3D_E_PARAM, "neo_fft3d: null argument");
+  std::lock_guard<std::mutex> lk(P->mu);
+  Slot* s = find_slot(P, n);
+  if (!s) return fail(FFT3D_E_FRAME, "neo_fft3d: frame " + std::to_string(n) + " is not cached");
+  CK(cudaSetDevice(P->device), "cudaSetDevice");
+  CK(cudaStreamSynchronize(P->stream), "synchronize");
+  CK(cudaMemcpy(out, s->spec, P->spec_elems() * sizeof(float2), cudaMemcpyDeviceToHost), "spectrum download");
+  return FFT3D_OK;
+}
+
+int fft3d_plane_geometry(fft3d_plane* P, int out[8]) {
+  if (!P || !out) return fail(FFT3D_E_PARAM, "neo_fft3d: null argument");
+  out[0] = P->g.nox; out[1] = P->g.noy;
+  out[2] = P->g.nox * P->g.sx + P->g.ow; out[3] = P->g.noy * P->g.sy + P->g.oh;
+  out[4] = P->g.nh; out[5] = P->g.nblocks; out[6] = P->g.ow; out[7] = P->g.oh;
+  return FFT3D_OK;
+}
+
+// Estimate the noise pattern from one frame (host memory), as the reference
+// does from frame pframe on its first GetFrame (src/fft3d_engine.h:485-504).
+int fft3d_plane_set_pattern_frame(fft3d_plane* P, const void* src, int stride) {
+  if (!P || !src) return fail(FFT3D_E_PARAM, "neo_fft3d: null argument");
+  std::lock_guard<std::mutex> lk(P->mu);
+  if (!P->pattern) return FFT3D_OK;
+  CK(cudaSetDevice(P->device), "cudaSetDevice");
+  Slot* s = evict_slot(P, 1, 0);
+  s->frame = -1;
+  CK(cudaMemcpy2DAsync(P->d_in, P->in_pitch, src, stride, (size_t)P->d.width * P->bytes, P->d.height,
+                       cudaMemcpyHostToDevice, P->stream), "frame upload");
+  int rc = launch_forward(P, P->d_in, (long long)P->in_pitch, s->spec, P->stream);
+  if (rc) return rc;
+  std::vector<float2> spec(P->spec_elems());
+  CK(cudaMemcpyAsync(spec.data(), s->spec, spec.size() * sizeof(float2), cudaMemcpyDeviceToHost, P->stream),
+     "spectrum download");
+  CK(cudaStreamSynchronize(P->stream), "synchronize");
+  estimate_pattern(P, spec);
+  rc = upload_pattern(P, P->d_pattern2d, P->h_pattern2d);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(P->stream), "synchronize");
+  P->pattern_set = true;
+  P->pattern3d_init = false;
+  return FFT3D_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,109 @@
+// Device kernels of the FFT3D filtering core (sm_100a, FP32 CUDA-core path).
+//
+// Per plane and output frame the hot path is three kernels:
+//   k_forward         frame -> mirrored cover -> windowed overlapped blocks ->
+//                     2D r2c FFT -> one slot of the device spectrum ring
+//                     (replaces FrameToCover + CoverToOverlap + FFTW r2c,
+//                     src/buffer.cpp:6-379, src/fft3d_engine.h:616-618,661-664)
+//   k_filter_inverse  Wiener 2D / 3D2..3D5, Kalman or sharpen-only filter of
+//                     every bin, sharpen/dehalo, 2D c2r -> time-domain blocks
+//                     (replaces Apply*/Kalman/Sharpen C kernels and FFTW c2r,
+//                     src/code_impl/*.cpp, src/fft3d_engine.h:669-674)
+//   k_overlap_add     synthesis window, overlap-add, rounding and clamped
+//                     8/16-bit (or float) write-back of the plane interior
+//                     (replaces OverlapToCover + CoverToFrame, src/buffer.cpp:382-600)
+//
+// One warp owns one block in the two FFT kernels; its tiles are staged in
+// shared memory so that every global access is coalesced.
+#pragma once
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace fft3d {
+
+// Geometry of one plane (after crop), see src/fft3d_engine.h:115-136.
+struct Geom {
+  int W, H;          // processed (cropped) plane size in pixels
+  int nox, noy;      // blocks per row / column (incl. the one-block mirror margin)
+  int nblocks;
+  int bw, bh, ow, oh;
+  int sx, sy;        // block step bw-ow, bh-oh (= mirror margins mirw, mirh)
+  int nh;            // bw/2 + 1
+  int interlaced;
+};
+
+// Per-plane constant tables on the device.
+struct Tables {
+  const float* wan_x;   // [bw] analysis window along x (wanxl | 1 | wanxr)
+  const float* wan_y;   // [bh]
+  const float* wsyn_xl; // [ow] synthesis windows, src/fft3d_engine.h:223-233
+  const float* wsyn_xr;
+  const float* wsyn_yl; // [oh]
+  const float* wsyn_yr;
+  const float2* grid;   // [bh*nh] gridsample, src/fft3d_engine.h:380-404
+  const float* wsharpen;  // [bh*nh]
+  const float* wdehalo;   // [bh*nh]
+  const float* pattern2d; // [bh*nh]
+  const float* pattern3d; // [bh*nh]
+};
+
+// Scalar filter constants, src/fft3d_engine.h:584-607.
+struct FilterConsts {
+  float sigma2n;      // btcur * sigma^2 / norm
+  float sigma2n_2d;   // sigma^2 / norm (Kalman)
+  float lowlimit;     // (beta - 1) / beta
+  float degrid;
+  float sharpen, dehalo;
+  float smin2n, smax2n, ht2n;
+  float kratio2;
+  int pattern;        // use pattern2d / pattern3d instead of sigma
+  int do_sharpen;     // run the separate sharpen/dehalo pass
+  int fuse_sharpen;   // 2D only: sharpen/dehalo factors inside the Wiener factor
+  int use_sharpen, use_dehalo;
+};
+
+struct ForwardArgs {
+  Geom g;
+  const void* src;        // frame plane at the crop origin
+  long long src_stride;   // bytes
+  float base;             // 2^(bits-1) for integer chroma, else 0
+  const float* wan_x;
+  const float* wan_y;
+  float2* spec;           // blocks x bh x nh
+};
+
+struct InverseArgs {
+  Geom g;
+  Tables t;
+  FilterConsts c;
+  const float2* in[5];    // spectra of frames n-2..n+2 (null when unused)
+  float2* kal_last;       // Kalman state: filtered spectrum of the previous frame
+  float* kal_covar;       // covariance (identical for re and im, src/code_impl/Kalman.cpp:41-64)
+  float* kal_covarp;      // process covariance
+  float* tdom;            // blocks x bh x bw time-domain output
+};
+
+struct OlaArgs {
+  Geom g;
+  Tables t;
+  const float* tdom;
+  void* dst;              // plane at the crop origin
+  long long dst_stride;   // bytes
+  float norm;
+  float rounder;          // 0.5 for integer formats, 0 for float
+  float base;
+  int maxval;             // (1 << bits) - 1
+};
+
+// Host-side launchers (fft3d_kernels.cu). They return cudaGetLastError().
+cudaError_t launch_forward(const ForwardArgs& a, int bytes_per_sample, cudaStream_t s);
+cudaError_t launch_filter_inverse(const InverseArgs& a, int mode, cudaStream_t s);
+cudaError_t launch_overlap_add(const OlaArgs& a, int bytes_per_sample, cudaStream_t s);
+bool block_size_supported(int bw, int bh);
+cudaError_t upload_twiddles();  // every registered size, on the current device
+
+// filter modes of launch_filter_inverse
+enum { MODE_SHARPEN_ONLY = -1, MODE_KALMAN = 0, MODE_WIENER2D = 1 /* 2..5: Wiener 3D with that many frames */ };
+
+}  // namespace fft3d

@@ -1,0 +1,22 @@
+// Table of the block sizes compiled into the library. Each kern_*.cu
+// translation unit instantiates the kernels of a few sizes and registers them
+// here at load time (FFT3D_REGISTER_SIZE in fft3d_kernels_impl.cuh).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "fft3d_kernels.cuh"
+
+namespace fft3d {
+
+struct SizeEntry {
+  int bw, bh;
+  cudaError_t (*fwd)(const ForwardArgs&, int bytes_per_sample, cudaStream_t);
+  cudaError_t (*inv)(const InverseArgs&, int mode, cudaStream_t);
+  cudaError_t (*upload)();  // the translation unit's twiddle table, once per device
+};
+
+bool register_size(const SizeEntry& e);
+const SizeEntry* find_size(int bw, int bh);
+int registered_sizes(SizeEntry* out, int max);
+
+}  // namespace fft3d

@@ -1,0 +1,150 @@
+"""Python binding of the C ABI in include/fft3d_b200.h (lib/libfft3d_b200.so).
+
+This is a thin ctypes layer: all work runs in the sm_100a kernels of the
+library. There is no CPU fallback; if the library or a CUDA device is missing,
+every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .params import FFT3DParams, PlaneDesc, make_params, plane_descs, processed_planes
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libfft3d_b200.so")
+_lib = None
+
+SYMBOLS = ("fft3d_params_default", "fft3d_plane_create", "fft3d_plane_filter", "fft3d_plane_filter_device",
+           "fft3d_plane_cached", "fft3d_plane_spectrum", "fft3d_plane_geometry", "fft3d_plane_set_pattern_frame",
+           "fft3d_plane_reset", "fft3d_plane_destroy", "fft3d_last_error", "fft3d_kernel_launches")
+
+
+class FFT3DError(RuntimeError):
+    pass
+
+
+def lib():
+    """Load the native library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FFT3DError(f"neo_fft3d_b200 native library not built: {LIB_PATH}")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, ci = ctypes.c_void_p, ctypes.c_int
+        L.fft3d_params_default.argtypes = [ctypes.POINTER(FFT3DParams)]
+        L.fft3d_plane_create.argtypes = [ctypes.POINTER(FFT3DParams), ctypes.POINTER(PlaneDesc), ci,
+                                         ctypes.POINTER(vp)]
+        L.fft3d_plane_filter.argtypes = [vp, ci, ctypes.POINTER(vp), ctypes.POINTER(ci), vp, ci]
+        L.fft3d_plane_filter_device.argtypes = [vp, ci, ctypes.POINTER(vp), ctypes.POINTER(ci), vp, ci, vp]
+        L.fft3d_plane_cached.argtypes = [vp, ci]
+        L.fft3d_plane_spectrum.argtypes = [vp, ci, vp]
+        L.fft3d_plane_geometry.argtypes = [vp, ctypes.POINTER(ci)]
+        L.fft3d_plane_set_pattern_frame.argtypes = [vp, vp, ci]
+        L.fft3d_plane_reset.argtypes = [vp]
+        L.fft3d_plane_destroy.argtypes = [vp]
+        L.fft3d_last_error.restype = ctypes.c_char_p
+        L.fft3d_kernel_launches.restype = ctypes.c_uint64
+        _lib = L
+    return _lib
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise FFT3DError(f"{lib().fft3d_last_error().decode()} (status {rc})")
+
+
+def kernel_launches() -> int:
+    return int(lib().fft3d_kernel_launches())
+
+
+class PlaneEngine:
+    """One GPU plane engine (the counterpart of the reference's FFT3DEngine)."""
+
+    def __init__(self, params: FFT3DParams, desc: PlaneDesc, device: int = 0):
+        self.params, self.desc = params, desc
+        h = ctypes.c_void_p()
+        _check(lib().fft3d_plane_create(ctypes.byref(params), ctypes.byref(desc), device, ctypes.byref(h)))
+        self.h = h
+        g = (ctypes.c_int * 8)()
+        _check(lib().fft3d_plane_geometry(self.h, g))
+        self.nox, self.noy, self.coverw, self.coverh, self.outwidth, self.nblocks, self.ow, self.oh = list(g)
+
+    def filter(self, n: int, window, out: np.ndarray) -> np.ndarray:
+        """Filter frame n from host arrays. window: frames n-2..n+2 (None where
+        absent or already cached); out: the output plane (written in place)."""
+        ptrs = (ctypes.c_void_p * 5)()
+        strides = (ctypes.c_int * 5)()
+        keep = []
+        for i, a in enumerate(window):
+            if a is not None:
+                a = np.ascontiguousarray(a)
+                keep.append(a)
+                ptrs[i] = a.ctypes.data
+                strides[i] = a.strides[0]
+        _check(lib().fft3d_plane_filter(self.h, n, ptrs, strides, out.ctypes.data, out.strides[0]))
+        return out
+
+    def filter_device(self, n: int, ptrs, strides, dst_ptr: int, dst_stride: int, stream: int = 0):
+        """Filter frame n from device pointers (ints); queued on `stream`."""
+        p = (ctypes.c_void_p * 5)(*[x or None for x in ptrs])
+        s = (ctypes.c_int * 5)(*strides)
+        _check(lib().fft3d_plane_filter_device(self.h, n, p, s, ctypes.c_void_p(dst_ptr), dst_stride,
+                                               ctypes.c_void_p(stream) if stream else None))
+
+    def cached(self, n: int) -> bool:
+        return bool(lib().fft3d_plane_cached(self.h, n))
+
+    def spectrum(self, n: int) -> np.ndarray:
+        buf = np.empty((self.nblocks, self.params.bh, self.outwidth, 2), np.float32)
+        _check(lib().fft3d_plane_spectrum(self.h, n, buf.ctypes.data))
+        return buf[..., 0] + 1j * buf[..., 1].astype(np.complex64)
+
+    def set_pattern_frame(self, frame: np.ndarray):
+        frame = np.ascontiguousarray(frame)
+        _check(lib().fft3d_plane_set_pattern_frame(self.h, frame.ctypes.data, frame.strides[0]))
+
+    def reset(self):
+        _check(lib().fft3d_plane_reset(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fft3d_plane_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def filter_clip(planes, frames=None, bits=None, device: int = 0, **kw):
+    """FFT3D(clip, **kw) on the GPU for a clip given as a list of [F,H,W] host
+    planes, the way the plugin drives its engines: one engine per processed
+    plane, frames in order, unprocessed planes copied. Returns output planes."""
+    F = planes[0].shape[0]
+    if bits is None:
+        bits = 8 if planes[0].dtype == np.uint8 else (32 if planes[0].dtype == np.float32 else 16)
+    p = make_params(**kw)
+    descs = plane_descs([a.shape[1:] for a in planes], bits, F)
+    proc = processed_planes(len(planes), kw.get("planes"), kw.get("y"), kw.get("u"), kw.get("v"))
+    frames = list(range(F)) if frames is None else list(frames)
+    outs = []
+    for i, a in enumerate(planes):
+        o = np.empty((len(frames),) + a.shape[1:], a.dtype)
+        if not proc[i]:
+            o[:] = a[frames]
+            outs.append(o)
+            continue
+        eng = PlaneEngine(p, descs[i], device)
+        if p.pfactor != 0:
+            eng.set_pattern_frame(a[min(max(p.pframe, 0), F - 1)])
+        for j, n in enumerate(frames):
+            win = [a[n + d] if 0 <= n + d < F else None for d in range(-2, 3)]
+            eng.filter(n, win, o[j])
+        eng.close()
+        outs.append(o)
+    return outs
