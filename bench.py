@@ -1,0 +1,354 @@
+#!/usr/bin/env python
+"""Benchmark of the FFT3D filtering core on B200.
+
+Workload (the configuration the headline metric is quoted on): 120 frames of
+seeded synthetic 8-bit YUV420 at 1920x1080 (sum-of-sinusoids field moving by
+<= 2 px/frame, Gaussian noise sigma 6), filtered with bt=5, sigma=3,
+bw=bh=32, ow=oh=16, sharpen=0.3 (all three planes, degrid=1 default).
+
+One step = the whole 120-frame clip filtered end to end (all planes, every
+output frame, edge frames with bt=1 as the reference does), inputs resident
+in HBM. The clip (373 MB) and the spectrum ring (~350 MB) are larger than L2,
+so no flush is needed between steps.
+
+Lines printed (rank 0, one JSON line):
+  value      frames/s of the device-resident path (whole job over N ranks)
+  e2e        frames/s through the C ABI with host buffers (pinned), copies in
+  roofline   the dominant kernel's algorithmic bytes / its CUDA-event time
+  cpu_baseline  the reference plugin (built from its sources, oracle/_ref) on
+             a bounded sample of the same workload on this host's cores
+``--impl reference`` times only the reference's CPU implementation.
+Multi-GPU (torchrun): independent replicas, one clip per rank, no collective
+on the data path ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+from neo_fft3d_b200 import synth  # noqa: E402
+
+WORKLOAD = "1080p_bt5_bw32"
+METRIC = "1080p bt=5 frames/s (120-frame YUV420 8-bit clip, bw=bh=32, ow=oh=16, sharpen=0.3)"
+UNIT = "frames/s"
+
+
+def workload():
+    w = synth.WORKLOADS[WORKLOAD]
+    return w["clip"], w["filt"]
+
+
+def canonical_frame_bytes(width, height, nblocks_total, bh, nh, bt):
+    """Cached-spectrum byte model per output frame: P_in + S + bt*S + P_out
+    (P = pixel bytes of all planes, S = unpadded FP32 complex half-spectra of
+    all blocks of all planes)."""
+    P = width * height * 3 // 2
+    S = nblocks_total * bh * nh * 8
+    return P + S + bt * S + P
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        rows = [r.split(",") for r in out.strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_reference(clip_kw, filt, frames, threads, first=10):
+    """Reference plugin (oracle/_ref) rendering `frames` output frames with
+    `threads` host threads, opt=0 (its SIMD path), ncpu=1. Returns seconds."""
+    from oracle import reference
+    planes = clip_kw["planes"]
+    c = reference.core()
+    clip = c.clip(planes)
+    node = c.invoke("neo_fft3d", "FFT3D", clip, opt=0, ncpu=1, **filt)
+    t = time.perf_counter()
+    node.render(first=first, count=frames, threads=threads)
+    secs = time.perf_counter() - t
+    del node, clip  # frees the reference's engines and spectrum caches
+    import gc
+    gc.collect()
+    return secs
+
+
+def reference_arm(args, rank):
+    clip_kw, filt = workload()
+    if rank != 0:
+        return None
+    planes = synth.make_clip(**clip_kw)
+    threads = os.cpu_count() or 1
+    # size the per-step sample so that the whole run stays within ~3 minutes
+    t1 = run_reference({"planes": planes}, filt, threads, threads)
+    per_frame = t1 / threads
+    budget = 150.0
+    frames = int(max(1, min(clip_kw["frames"] - 20, budget / max(1, args.steps + args.warmup) / per_frame)))
+    for _ in range(args.warmup):
+        run_reference({"planes": planes}, filt, frames, threads)
+    total = 0.0
+    for _ in range(args.steps):
+        total += run_reference({"planes": planes}, filt, frames, threads)
+    fps = args.steps * frames / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": fps, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "frames_per_step": frames, "opt": 0, "ncpu": 1, "host_threads": threads},
+        "cpu_baseline": {"value": fps, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{frames} output frames (of 120) of the 1080p bt=5 clip per step, "
+                                   f"{threads} host threads (frame-parallel), opt=0, FFT = project FFTW-API shim"},
+        "e2e": {"value": fps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        # the reference is a CPU implementation: rank 0 runs it, others exit
+        line = reference_arm(args, rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    from neo_fft3d_b200 import engine
+    from neo_fft3d_b200.params import make_params, plane_descs
+
+    clip_kw, filt = workload()
+    F = clip_kw["frames"]
+    planes = synth.make_clip(**clip_kw)
+    p = make_params(**filt)
+    descs = plane_descs([a.shape[1:] for a in planes], 8, F)
+    dev = [torch.from_numpy(a).cuda() for a in planes]
+    outs = [torch.empty_like(d) for d in dev]
+    engs = [engine.PlaneEngine(p, d, local) for d in descs]
+    streams = [torch.cuda.Stream() for _ in engs]
+    master = torch.cuda.current_stream()
+
+    def step():
+        ev = torch.cuda.Event()
+        ev.record(master)
+        for i, e in enumerate(engs):
+            s = streams[i]
+            s.wait_event(ev)
+            a, o = dev[i], outs[i]
+            W = a.shape[2]
+            fb = a.shape[1] * W
+            base = a.data_ptr()
+            obase = o.data_ptr()
+            for n in range(F):
+                ptrs = [base + (n + d) * fb if 0 <= n + d < F else 0 for d in range(-2, 3)]
+                e.filter_device(n, ptrs, [W] * 5, obase + n * fb, W, s.cuda_stream)
+        for s in streams:
+            master.wait_stream(s)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = engine.kernel_launches()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0.record(master)
+    for _ in range(args.steps):
+        step()
+    t1.record(master)
+    torch.cuda.synchronize()
+    launches = engine.kernel_launches() - l0
+    clk = clocks.stop()
+    ms = t0.elapsed_time(t1)
+    if world > 1:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+        dist.barrier()
+    ms_per_step = ms / args.steps
+    value = world * F * args.steps / (ms / 1000.0)
+
+    # per-kernel roofline from an instrumented pass (events around each launch)
+    for e in engs:
+        e.set_timing(True)
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    per = {}
+    for e in engs:
+        for k, (n, msk, b) in e.timing().items():
+            c = per.setdefault(k, [0.0, 0.0, 0.0])
+            c[0] += n; c[1] += msk; c[2] += b
+        e.set_timing(False)
+    dom = max(per, key=lambda k: per[k][1])
+    n_l, ms_l, b_l = per[dom]
+    peak, peak_kind = load_peaks()
+    achieved = (b_l / n_l) / (ms_l / n_l / 1000.0) / 1e9
+    traffic = load_traffic().get(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": traffic, "algorithmic_bytes_per_launch": b_l / n_l,
+                "avg_launch_us": 1000.0 * ms_l / n_l,
+                "kernel_share": {k: v[1] / sum(x[1] for x in per.values()) for k, v in per.items()}}
+    nblocks_total = sum(e.nblocks for e in engs)
+    fb_bytes = canonical_frame_bytes(clip_kw["width"], clip_kw["height"], nblocks_total, p.bh, p.bw // 2 + 1, p.bt)
+    frame_roofline = {"bytes_per_frame": fb_bytes, "achieved_gbs": fb_bytes * value / world / 1e9,
+                      "frac": fb_bytes * value / world / 1e9 / peak}
+
+    # end to end through the C ABI with pinned host buffers (one host thread per plane)
+    host_in = [torch.from_numpy(a).pin_memory() for a in planes]
+    host_out = [torch.empty_like(h).pin_memory() for h in host_in]
+    nps_in = [h.numpy() for h in host_in]
+    nps_out = [h.numpy() for h in host_out]
+
+    def e2e_plane(i):
+        e, a, o = engs[i], nps_in[i], nps_out[i]
+        e.reset()
+        for n in range(F):
+            win = [a[n + d] if 0 <= n + d < F else None for d in range(-2, 3)]
+            e.filter(n, win, o[n])
+
+    def e2e_step():
+        th = [threading.Thread(target=e2e_plane, args=(i,)) for i in range(len(engs))]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+
+    e2e = None
+    if args.e2e_steps > 0:
+        e2e_step()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t
+        if world > 1:
+            tt = torch.tensor([e2e_s], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e2e_s = float(tt.item())
+        frame_bytes = sum(a[0].nbytes for a in planes)
+        e2e = {"value": world * F * args.e2e_steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": F * frame_bytes, "d2h_bytes_per_step": F * frame_bytes,
+               "path": "fft3d_plane_filter (host API), one host thread per plane, pinned buffers"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            threads = os.cpu_count() or 1
+            sample = 2 * threads
+            secs = run_reference({"planes": planes}, filt, sample, threads)
+            cpu = {"value": sample / secs, "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"{sample} output frames (frames 10..{10 + sample - 1}) of the same clip, "
+                             f"{threads} host threads, opt=0, ncpu=1, FFT = project FFTW-API shim"}
+        except Exception as ex:  # the reference build is optional on a box
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {ex}"}
+
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "frames_per_step": F, "width": 1920, "height": 1080,
+                       "format": "YUV420P8", "bt": 5, "sigma": 3.0, "bw": 32, "bh": 32, "ow": 16, "oh": 16,
+                       "sharpen": 0.3, "path": "plain_fp32", "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (373 MB clip + ~350 MB spectrum ring per rank), no flush"},
+            "roofline": roofline, "frame_roofline": frame_roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "clocks": clk, "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    for e in engs:
+        e.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -113,6 +113,17 @@ int fft3d_plane_reset(fft3d_plane* h);
 
 void fft3d_plane_destroy(fft3d_plane* h);
 
+/* Per-kernel timing of this handle: when enabled, every launch is bracketed
+ * by CUDA events on the stream it runs on. */
+int fft3d_plane_set_timing(fft3d_plane* h, int enable);
+
+/* Read and reset the timing counters: out[3k+0] launches, out[3k+1] summed
+ * event milliseconds, out[3k+2] summed algorithmic bytes (what the launch's
+ * interface must read and write once), for k = 0 forward (gather + window +
+ * r2c), 1 filter + inverse (spectra in, time-domain blocks out), 2 overlap-add
+ * (time-domain blocks in, pixels out). Waits for the recorded launches. */
+int fft3d_plane_timing(fft3d_plane* h, double out[9]);
+
 /* Message of the last failure on this thread ("" if none). */
 const char* fft3d_last_error(void);
 

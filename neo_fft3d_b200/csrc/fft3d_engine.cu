@@ -47,6 +47,15 @@ struct Slot {
   uint64_t stamp = 0;
 };
 
+// Optional per-kernel timing: CUDA events recorded on the launching stream
+// around every launch, resolved when the counters are read.
+enum { K_FORWARD = 0, K_INVERSE = 1, K_OLA = 2, K_COUNT = 3 };
+struct Timed {
+  int kind;
+  double bytes;
+  cudaEvent_t a, b;
+};
+
 }  // namespace
 
 struct fft3d_plane {
@@ -78,10 +87,47 @@ struct fft3d_plane {
   size_t in_pitch = 0;
   void* d_out = nullptr;  // staging of the host output (whole plane)
   size_t out_pitch = 0;
+  bool timing = false;
+  std::vector<Timed> pending;
+  std::vector<cudaEvent_t> event_pool;
+  double t_launches[K_COUNT] = {0, 0, 0}, t_ms[K_COUNT] = {0, 0, 0}, t_bytes[K_COUNT] = {0, 0, 0};
   size_t spec_elems() const { return (size_t)g.nblocks * g.bh * g.nh; }
 };
 
 namespace {
+
+cudaEvent_t take_event(fft3d_plane* P) {
+  if (!P->event_pool.empty()) {
+    cudaEvent_t e = P->event_pool.back();
+    P->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Brackets one launch with events when timing is on; `bytes` is the launch's
+// algorithmic traffic (what its interface must read and write once).
+struct TimeScope {
+  fft3d_plane* P;
+  int kind;
+  double bytes;
+  cudaStream_t st;
+  cudaEvent_t a = nullptr;
+  TimeScope(fft3d_plane* p, int k, double b, cudaStream_t s) : P(p), kind(k), bytes(b), st(s) {
+    if (P->timing) {
+      a = take_event(P);
+      cudaEventRecord(a, st);
+    }
+  }
+  ~TimeScope() {
+    if (!a) return;
+    cudaEvent_t b = take_event(P);
+    cudaEventRecord(b, st);
+    P->pending.push_back(Timed{kind, bytes, a, b});
+  }
+};
 
 // ---------------------------------------------------------------- tables
 // Same formulas as the reference's constructor (src/fft3d_engine.h:204-375),
@@ -183,6 +229,8 @@ void free_plane(fft3d_plane* P) {
   if (!P) return;
   cudaSetDevice(P->device);
   if (P->stream) cudaStreamSynchronize(P->stream);
+  for (auto& t : P->pending) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
+  for (auto e : P->event_pool) cudaEventDestroy(e);
   for (auto& s : P->slots) cudaFree(s.spec);
   cudaFree(P->d_tables);
   cudaFree(P->d_tdom);
@@ -225,6 +273,7 @@ int launch_forward(fft3d_plane* P, const void* plane, long long stride, float2* 
   a.wan_x = P->d_wan_x;
   a.wan_y = P->d_wan_y;
   a.spec = spec;
+  TimeScope ts(P, K_FORWARD, (double)P->g.W * P->g.H * P->bytes + (double)P->spec_elems() * sizeof(float2), st);
   CK(fft3d::launch_forward(a, P->bytes, st), "forward kernel");
   g_launches++;
   return FFT3D_OK;
@@ -319,7 +368,14 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
   ia.kal_covar = P->d_cov;
   ia.kal_covarp = P->d_covp;
   ia.tdom = P->d_tdom;
-  CK(fft3d::launch_filter_inverse(ia, mode, st), "filter/inverse kernel");
+  {
+    // reads: the spectra of the window (Kalman: + state read and written);
+    // writes: the time-domain blocks
+    const double S = (double)P->spec_elems() * sizeof(float2);
+    const double state = bt == 0 ? 2.0 * (double)P->spec_elems() * 16 : 0.0;
+    TimeScope ts(P, K_INVERSE, (to - from + 1) * S + state + (double)P->g.nblocks * P->g.bh * P->g.bw * 4, st);
+    CK(fft3d::launch_filter_inverse(ia, mode, st), "filter/inverse kernel");
+  }
   g_launches++;
   // output: the crop borders come from the source frame (src/fft3d.hpp:292-352)
   const bool crop = ep.l > 0 || ep.t > 0 || ep.r > 0 || ep.b > 0;
@@ -350,7 +406,10 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
   oa.rounder = ints ? 0.5f : 0.f;
   oa.base = (ints && P->d.is_chroma) ? (float)(1 << (P->d.bits - 1)) : 0.f;
   oa.maxval = P->bytes == 1 ? 255 : (1 << P->d.bits) - 1;
-  CK(fft3d::launch_overlap_add(oa, P->bytes, st), "overlap-add kernel");
+  {
+    TimeScope ts(P, K_OLA, (double)P->g.nblocks * P->g.bh * P->g.bw * 4 + (double)P->g.W * P->g.H * P->bytes, st);
+    CK(fft3d::launch_overlap_add(oa, P->bytes, st), "overlap-add kernel");
+  }
   g_launches++;
   if (host) {
     char* hdst = static_cast<char*>(dst) + (size_t)P->t * dst_stride + (size_t)P->l * P->bytes;
@@ -636,6 +695,37 @@ int fft3d_plane_set_pattern_frame(fft3d_plane* P, const void* src, int stride) {
   CK(cudaStreamSynchronize(P->stream), "synchronize");
   P->pattern_set = true;
   P->pattern3d_init = false;
+  return FFT3D_OK;
+}
+
+int fft3d_plane_set_timing(fft3d_plane* P, int enable) {
+  if (!P) return fail(FFT3D_E_PARAM, "neo_fft3d: null handle");
+  std::lock_guard<std::mutex> lk(P->mu);
+  P->timing = enable != 0;
+  return FFT3D_OK;
+}
+
+int fft3d_plane_timing(fft3d_plane* P, double out[9]) {
+  if (!P || !out) return fail(FFT3D_E_PARAM, "neo_fft3d: null argument");
+  std::lock_guard<std::mutex> lk(P->mu);
+  CK(cudaSetDevice(P->device), "cudaSetDevice");
+  for (auto& t : P->pending) {
+    CK(cudaEventSynchronize(t.b), "event synchronize");
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, t.a, t.b), "event elapsed time");
+    P->t_launches[t.kind] += 1;
+    P->t_ms[t.kind] += ms;
+    P->t_bytes[t.kind] += t.bytes;
+    P->event_pool.push_back(t.a);
+    P->event_pool.push_back(t.b);
+  }
+  P->pending.clear();
+  for (int k = 0; k < K_COUNT; k++) {
+    out[3 * k] = P->t_launches[k];
+    out[3 * k + 1] = P->t_ms[k];
+    out[3 * k + 2] = P->t_bytes[k];
+    P->t_launches[k] = P->t_ms[k] = P->t_bytes[k] = 0;
+  }
   return FFT3D_OK;
 }
 

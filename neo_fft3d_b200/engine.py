@@ -19,7 +19,9 @@ _lib = None
 
 SYMBOLS = ("fft3d_params_default", "fft3d_plane_create", "fft3d_plane_filter", "fft3d_plane_filter_device",
            "fft3d_plane_cached", "fft3d_plane_spectrum", "fft3d_plane_geometry", "fft3d_plane_set_pattern_frame",
-           "fft3d_plane_reset", "fft3d_plane_destroy", "fft3d_last_error", "fft3d_kernel_launches")
+           "fft3d_plane_reset", "fft3d_plane_destroy", "fft3d_last_error", "fft3d_kernel_launches",
+           "fft3d_plane_set_timing", "fft3d_plane_timing")
+KERNELS = ("forward", "filter_inverse", "overlap_add")
 
 
 class FFT3DError(RuntimeError):
@@ -47,6 +49,8 @@ def lib():
         L.fft3d_plane_destroy.argtypes = [vp]
         L.fft3d_last_error.restype = ctypes.c_char_p
         L.fft3d_kernel_launches.restype = ctypes.c_uint64
+        L.fft3d_plane_set_timing.argtypes = [vp, ci]
+        L.fft3d_plane_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         _lib = L
     return _lib
 
@@ -105,6 +109,15 @@ class PlaneEngine:
     def set_pattern_frame(self, frame: np.ndarray):
         frame = np.ascontiguousarray(frame)
         _check(lib().fft3d_plane_set_pattern_frame(self.h, frame.ctypes.data, frame.strides[0]))
+
+    def set_timing(self, enable: bool):
+        _check(lib().fft3d_plane_set_timing(self.h, 1 if enable else 0))
+
+    def timing(self) -> dict:
+        """{kernel: (launches, milliseconds, algorithmic bytes)}; resets the counters."""
+        out = (ctypes.c_double * 9)()
+        _check(lib().fft3d_plane_timing(self.h, out))
+        return {k: (out[3 * i], out[3 * i + 1], out[3 * i + 2]) for i, k in enumerate(KERNELS)}
 
     def reset(self):
         _check(lib().fft3d_plane_reset(self.h))

@@ -79,7 +79,7 @@ def make_clip(width: int, height: int, frames: int, *, bits: int = 8, noise_sigm
             if with_clean:
                 carr[t] = np.clip(np.rint(v), 0, maxv).astype(dtype)
             if noise_sigma > 0:
-                v = v + noise_rng.standard_normal((h, w)) * noise_sigma
+                v = v + noise_rng.standard_normal((h, w), dtype=np.float32) * np.float32(noise_sigma)
             arr[t] = np.clip(np.rint(v), 0, maxv).astype(dtype)
         out.append(arr)
         if with_clean:
