@@ -207,11 +207,11 @@ def main():
     streams = [torch.cuda.Stream() for _ in engs]
     master = torch.cuda.current_stream()
 
-    def step():
+    def step(serial=False):
         ev = torch.cuda.Event()
         ev.record(master)
         for i, e in enumerate(engs):
-            s = streams[i]
+            s = master if serial else streams[i]
             s.wait_event(ev)
             a, o = dev[i], outs[i]
             W = a.shape[2]
@@ -250,11 +250,13 @@ def main():
     ms_per_step = ms / args.steps
     value = world * F * args.steps / (ms / 1000.0)
 
-    # per-kernel roofline from an instrumented pass (events around each launch)
+    # per-kernel roofline from an instrumented pass (events around each
+    # launch; planes serialised on one stream so that no other kernel shares
+    # the GPU during a timed launch)
     for e in engs:
         e.set_timing(True)
     for _ in range(3):
-        step()
+        step(serial=True)
     torch.cuda.synchronize()
     per = {}
     for e in engs:

@@ -121,8 +121,10 @@ int fft3d_plane_set_timing(fft3d_plane* h, int enable);
  * event milliseconds, out[3k+2] summed algorithmic bytes (what the launch's
  * interface must read and write once), for k = 0 forward (gather + window +
  * r2c), 1 filter + inverse (spectra in, time-domain blocks out), 2 overlap-add
- * (time-domain blocks in, pixels out). Waits for the recorded launches. */
-int fft3d_plane_timing(fft3d_plane* h, double out[9]);
+ * (time-domain blocks in, pixels out), 3 fused (newest frame's pixels and the
+ * older spectra in; newest spectrum and time-domain blocks out). Waits for the
+ * recorded launches. */
+int fft3d_plane_timing(fft3d_plane* h, double out[12]);
 
 /* Message of the last failure on this thread ("" if none). */
 const char* fft3d_last_error(void);

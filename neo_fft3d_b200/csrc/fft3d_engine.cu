@@ -7,6 +7,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -49,7 +50,7 @@ struct Slot {
 
 // Optional per-kernel timing: CUDA events recorded on the launching stream
 // around every launch, resolved when the counters are read.
-enum { K_FORWARD = 0, K_INVERSE = 1, K_OLA = 2, K_COUNT = 3 };
+enum { K_FORWARD = 0, K_INVERSE = 1, K_OLA = 2, K_FUSED = 3, K_COUNT = 4 };
 struct Timed {
   int kind;
   double bytes;
@@ -87,10 +88,14 @@ struct fft3d_plane {
   size_t in_pitch = 0;
   void* d_out = nullptr;  // staging of the host output (whole plane)
   size_t out_pitch = 0;
+  uint64_t frames_done = 0;
+  // steady-state kernel choice: k_fused (forward + filter + inverse in one
+  // launch) or k_forward then k_filter_inverse; NEO_FFT3D_FUSED=1 selects fused
+  bool fused = false;
   bool timing = false;
   std::vector<Timed> pending;
   std::vector<cudaEvent_t> event_pool;
-  double t_launches[K_COUNT] = {0, 0, 0}, t_ms[K_COUNT] = {0, 0, 0}, t_bytes[K_COUNT] = {0, 0, 0};
+  double t_launches[K_COUNT] = {}, t_ms[K_COUNT] = {}, t_bytes[K_COUNT] = {};
   size_t spec_elems() const { return (size_t)g.nblocks * g.bh * g.nh; }
 };
 
@@ -264,7 +269,7 @@ Slot* evict_slot(fft3d_plane* P, int lo, int hi) {
   return best;
 }
 
-int launch_forward(fft3d_plane* P, const void* plane, long long stride, float2* spec, cudaStream_t st) {
+fft3d::ForwardArgs forward_args(fft3d_plane* P, const void* plane, long long stride, float2* spec) {
   fft3d::ForwardArgs a;
   a.g = P->g;
   a.src = static_cast<const char*>(plane) + (long long)P->t * stride + (long long)P->l * P->bytes;
@@ -273,6 +278,11 @@ int launch_forward(fft3d_plane* P, const void* plane, long long stride, float2* 
   a.wan_x = P->d_wan_x;
   a.wan_y = P->d_wan_y;
   a.spec = spec;
+  return a;
+}
+
+int launch_forward(fft3d_plane* P, const void* plane, long long stride, float2* spec, cudaStream_t st) {
+  fft3d::ForwardArgs a = forward_args(P, plane, stride, spec);
   TimeScope ts(P, K_FORWARD, (double)P->g.W * P->g.H * P->bytes + (double)P->spec_elems() * sizeof(float2), st);
   CK(fft3d::launch_forward(a, P->bytes, st), "forward kernel");
   g_launches++;
@@ -330,14 +340,6 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
     return fail(FFT3D_E_PARAM, "neo_fft3d: noise pattern not estimated yet (fft3d_plane_set_pattern_frame)");
   const int from = bt > 0 && btcur > 1 ? -btcur / 2 : 0;
   const int to = bt > 0 && btcur > 1 ? (btcur - 1) / 2 : 0;
-  fft3d::InverseArgs ia{};
-  for (int d = from; d <= to; d++) {
-    Slot* s = nullptr;
-    int rc = spectrum_slot(P, n + d, n + from, n + to, src ? src[2 + d] : nullptr, stride ? stride[2 + d] : 0, host,
-                           st, &s);
-    if (rc) return rc;
-    ia.in[2 + d] = s->spec;
-  }
   if (bt > 0 && btcur > 1 && P->pattern && !P->pattern3d_init) {  // :625-630
     std::vector<float> p3(P->h_pattern2d.size());
     for (size_t i = 0; i < p3.size(); i++) p3[i] = P->h_pattern2d[i] * (float)btcur;
@@ -346,6 +348,38 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
     P->pattern3d_init = true;
   }
   const int mode = bt > 0 ? btcur : bt;
+  fft3d::InverseArgs ia{};
+  // The steady state computes one new spectrum per output frame, the newest
+  // of the window, in the fused kernel; older frames missing from the ring
+  // (clip start, seeks) are transformed first by the forward kernel.
+  const int newest = n + to;
+  const bool fused = P->fused && P->bytes != 4 && !find_slot(P, newest);
+  for (int d = from; d <= (fused ? to - 1 : to); d++) {
+    Slot* s = nullptr;
+    int rc = spectrum_slot(P, n + d, n + from, n + to, src ? src[2 + d] : nullptr, stride ? stride[2 + d] : 0, host,
+                           st, &s);
+    if (rc) return rc;
+    ia.in[2 + d] = s->spec;
+  }
+  Slot* news = nullptr;
+  const void* new_src = nullptr;
+  long long new_stride = 0;
+  if (fused) {
+    const void* plane = src ? src[2 + to] : nullptr;
+    if (!plane) return fail(FFT3D_E_FRAME, "neo_fft3d: frame " + std::to_string(newest) + " is needed but was not supplied");
+    news = evict_slot(P, n + from, n + to);
+    if (!news) return fail(FFT3D_E_PARAM, "neo_fft3d: spectrum ring too small");
+    news->frame = -1;
+    new_src = plane;
+    new_stride = stride[2 + to];
+    if (host) {
+      CK(cudaMemcpy2DAsync(P->d_in, P->in_pitch, plane, stride[2 + to], (size_t)P->d.width * P->bytes, P->d.height,
+                           cudaMemcpyHostToDevice, st), "frame upload");
+      new_src = P->d_in;
+      new_stride = (long long)P->in_pitch;
+    }
+    ia.in[2 + to] = news->spec;
+  }
   ia.g = P->g;
   ia.t = P->tab;
   fft3d::FilterConsts& c = ia.c;
@@ -368,13 +402,28 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
   ia.kal_covar = P->d_cov;
   ia.kal_covarp = P->d_covp;
   ia.tdom = P->d_tdom;
+  ia.reverse = (int)(P->frames_done++ & 1);
   {
-    // reads: the spectra of the window (Kalman: + state read and written);
-    // writes: the time-domain blocks
     const double S = (double)P->spec_elems() * sizeof(float2);
     const double state = bt == 0 ? 2.0 * (double)P->spec_elems() * 16 : 0.0;
-    TimeScope ts(P, K_INVERSE, (to - from + 1) * S + state + (double)P->g.nblocks * P->g.bh * P->g.bw * 4, st);
-    CK(fft3d::launch_filter_inverse(ia, mode, st), "filter/inverse kernel");
+    const double T = (double)P->g.nblocks * P->g.bh * P->g.bw * 4;
+    if (fused) {
+      // reads: the newest frame's pixels and the older spectra (+ Kalman state);
+      // writes: the newest spectrum and the time-domain blocks
+      fft3d::FusedArgs fa;
+      fa.f = forward_args(P, new_src, new_stride, news->spec);
+      fa.v = ia;
+      TimeScope ts(P, K_FUSED, (double)P->g.W * P->g.H * P->bytes + (to - from) * S + S + state + T, st);
+      CK(fft3d::launch_fused(fa, mode, P->bytes, st), "fused kernel");
+    } else {
+      // reads: the spectra of the window (+ Kalman state); writes: the time-domain blocks
+      TimeScope ts(P, K_INVERSE, (to - from + 1) * S + state + T, st);
+      CK(fft3d::launch_filter_inverse(ia, mode, st), "filter/inverse kernel");
+    }
+  }
+  if (fused) {
+    news->frame = newest;
+    news->stamp = ++P->clock;
   }
   g_launches++;
   // output: the crop borders come from the source frame (src/fft3d.hpp:292-352)
@@ -450,6 +499,10 @@ int fft3d_plane_create(const fft3d_params* p, const fft3d_plane_desc* d, int dev
   P->ep = *p;
   P->d = *d;
   P->device = device;
+  {
+    const char* f = std::getenv("NEO_FFT3D_FUSED");
+    P->fused = f && f[0] == '1';
+  }
   fft3d_params& ep = P->ep;
   if (d->bits < 8 || (d->bits > 16 && d->bits != 32)) { delete P; return fail(FFT3D_E_PARAM, "neo_fft3d: unsupported bit depth"); }
   P->bytes = d->bits <= 8 ? 1 : (d->bits <= 16 ? 2 : 4);
@@ -705,7 +758,7 @@ int fft3d_plane_set_timing(fft3d_plane* P, int enable) {
   return FFT3D_OK;
 }
 
-int fft3d_plane_timing(fft3d_plane* P, double out[9]) {
+int fft3d_plane_timing(fft3d_plane* P, double out[12]) {
   if (!P || !out) return fail(FFT3D_E_PARAM, "neo_fft3d: null argument");
   std::lock_guard<std::mutex> lk(P->mu);
   CK(cudaSetDevice(P->device), "cudaSetDevice");

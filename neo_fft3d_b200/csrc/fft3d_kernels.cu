@@ -123,6 +123,11 @@ cudaError_t launch_filter_inverse(const InverseArgs& a, int mode, cudaStream_t s
   return e ? e->inv(a, mode, s) : cudaErrorInvalidValue;
 }
 
+cudaError_t launch_fused(const FusedArgs& a, int mode, int bytes, cudaStream_t s) {
+  const SizeEntry* e = find_size(a.v.g.bw, a.v.g.bh);
+  return e ? e->fused(a, mode, bytes, s) : cudaErrorInvalidValue;
+}
+
 cudaError_t launch_overlap_add(const OlaArgs& a, int bytes, cudaStream_t s) {
   dim3 block(32, 8);
   dim3 grid((a.g.W + 31) / 32, (a.g.H + 7) / 8);

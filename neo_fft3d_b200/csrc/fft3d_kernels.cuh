@@ -82,6 +82,16 @@ struct InverseArgs {
   float* kal_covar;       // covariance (identical for re and im, src/code_impl/Kalman.cpp:41-64)
   float* kal_covarp;      // process covariance
   float* tdom;            // blocks x bh x bw time-domain output
+  int reverse;            // walk the blocks from the end (alternated per frame so
+                          // that the blocks read last stay in L2 for the next frame)
+};
+
+// Forward transform of the window's newest frame fused with the filter and
+// the inverse transform (k_fused). f.src/f.spec: the newest frame and its ring
+// slot; v.in[]: the window's spectra (the newest frame's entry is f.spec).
+struct FusedArgs {
+  ForwardArgs f;
+  InverseArgs v;
 };
 
 struct OlaArgs {
@@ -100,6 +110,8 @@ struct OlaArgs {
 cudaError_t launch_forward(const ForwardArgs& a, int bytes_per_sample, cudaStream_t s);
 cudaError_t launch_filter_inverse(const InverseArgs& a, int mode, cudaStream_t s);
 cudaError_t launch_overlap_add(const OlaArgs& a, int bytes_per_sample, cudaStream_t s);
+// cudaErrorNotSupported when no fused kernel exists for the sample type (float)
+cudaError_t launch_fused(const FusedArgs& a, int mode, int bytes_per_sample, cudaStream_t s);
 bool block_size_supported(int bw, int bh);
 cudaError_t upload_twiddles();  // every registered size, on the current device
 

@@ -11,7 +11,8 @@
 namespace fft3d {
 namespace {
 
-constexpr int kWarps = 4;  // warps (= blocks in flight) per CTA in the FFT kernels
+constexpr int kWarps = 4;       // warps per CTA in k_forward / k_filter_inverse
+constexpr int kFusedWarps = 2;  // warps (= blocks) per CTA in k_fused
 
 // reflect-101 of index s into [0, n): the cover's mirror margins
 // (src/buffer.cpp:19-26, 65-79); repeated for planes narrower than a margin.
@@ -41,59 +42,181 @@ __device__ __forceinline__ float load_sample<uint16_t>(const uint16_t* p) { retu
 template <>
 __device__ __forceinline__ float load_sample<float>(const float* p) { return __ldg(p); }
 
-template <int BW, int BH>
-__host__ __device__ constexpr int fft_smem_floats() {
-  return BH * (BW + 1) + BH * (BW / 2 + 1) * 2;
+// Blocks per warp of the FFT kernels: enough that the bw/2 column transforms
+// of all of them (DC and Nyquist columns share one complex transform) fill
+// the 32 lanes (2 for bw = 32, 4 for bw = 16, 1 for bw = 48).
+template <int BW>
+__host__ __device__ constexpr int blocks_per_warp() {
+  return (32 / (BW / 2)) < 1 ? 1 : ((32 / (BW / 2)) > 4 ? 4 : 32 / (BW / 2));
 }
+
+template <int BW, int BH>
+__host__ __device__ constexpr int fft_smem_bytes() {
+  return blocks_per_warp<BW>() * BH * (BW / 2 + 1) * 8;
+}
+
+// Row of BW samples starting at p, as floats; 16-byte vector loads when the
+// row is aligned (the common interior case), scalar loads otherwise.
+template <typename T, int BW>
+__device__ __forceinline__ void load_row(const T* p, float (&r)[BW]) {
+  constexpr int BYTES = BW * (int)sizeof(T);
+  if constexpr (BYTES % 16 == 0) {
+    if ((reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+      const uint4* q = reinterpret_cast<const uint4*>(p);
+#pragma unroll
+      for (int v = 0; v < BYTES / 16; v++) {
+        const uint4 u = __ldg(q + v);
+        const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+        constexpr int PER = 16 / (int)sizeof(T);
+#pragma unroll
+        for (int j = 0; j < PER; j++) {
+          float f;
+          if constexpr (sizeof(T) == 1) f = (float)((w[j >> 2] >> (8 * (j & 3))) & 0xffu);
+          else if constexpr (sizeof(T) == 2) f = (float)((w[j >> 1] >> (16 * (j & 1))) & 0xffffu);
+          else f = __uint_as_float(w[j]);
+          r[v * PER + j] = f;
+        }
+      }
+      return;
+    }
+  }
+#pragma unroll
+  for (int x = 0; x < BW; x++) r[x] = load_sample<T>(p + x);
+}
+
+// ---------------------------------------------------------------- block FFT phases
+// Sb points at one block's bh x (bw/2+1) complex tile in shared memory.
+
+// Row y of block `blk`: gather (mirrored at the plane edges), analysis window,
+// r2c along x into row y of Sb.
+template <int BW, int BH, typename T>
+__device__ __forceinline__ void fwd_row(const ForwardArgs& a, int blk, int y, float2* Sb) {
+  constexpr int NH = BW / 2 + 1;
+  const Geom& g = a.g;
+  const int by = blk / g.nox, bx = blk - by * g.nox;
+  const int k = reflect101(by * g.sy + y - g.sy, g.H);
+  const T* srow = reinterpret_cast<const T*>(static_cast<const char*>(a.src) +
+                                             (long long)field_row(k, g.H, g.interlaced) * a.src_stride);
+  const int x0 = bx * g.sx - g.sx;  // source column of block column 0
+  float r[BW];
+  if (x0 >= 0 && x0 + BW <= g.W) {
+    load_row<T, BW>(srow + x0, r);
+  } else {
+#pragma unroll
+    for (int x = 0; x < BW; x++) r[x] = load_sample<T>(srow + reflect101(x0 + x, g.W));
+  }
+  const float wy = __ldg(a.wan_y + y);
+#pragma unroll
+  for (int x = 0; x < BW; x++) r[x] = (r[x] - a.base) * __ldg(a.wan_x + x) * wy;
+  float2 c[NH];
+  rfft<BW>(r, c);
+  float2* row = Sb + y * NH;
+#pragma unroll
+  for (int kk = 0; kk < NH; kk++) row[kk] = c[kk];
+}
+
+// Column c (0 < c < bw/2) forward DFT along y in place; c == 0 transforms the
+// real columns 0 and bw/2 together as one complex sequence col0 + i colN.
+template <int BW, int BH>
+__device__ __forceinline__ void fwd_col(float2* Sb, int c) {
+  constexpr int NH = BW / 2 + 1, HC = BW / 2;
+  float2 col[BH];
+  if (c == 0) {
+#pragma unroll
+    for (int y = 0; y < BH; y++) col[y] = make_float2(Sb[y * NH].x, Sb[y * NH + HC].x);
+    cfft<BH, -1>(col);
+#pragma unroll
+    for (int h = 0; h < BH; h++) {
+      const float2 zh = col[h], zm = cconj(col[(BH - h) % BH]);
+      Sb[h * NH] = make_float2(0.5f * (zh.x + zm.x), 0.5f * (zh.y + zm.y));
+      const float2 d = csub(zh, zm);
+      Sb[h * NH + HC] = make_float2(0.5f * d.y, -0.5f * d.x);
+    }
+  } else {
+#pragma unroll
+    for (int y = 0; y < BH; y++) col[y] = Sb[y * NH + c];
+    cfft<BH, -1>(col);
+#pragma unroll
+    for (int h = 0; h < BH; h++) Sb[h * NH + c] = col[h];
+  }
+}
+
+// Column c inverse DFT along y in place; c == 0 handles columns 0 and bw/2
+// together (both Hermitian, so both inverses are real).
+template <int BW, int BH>
+__device__ __forceinline__ void inv_col(float2* Sb, int c) {
+  constexpr int NH = BW / 2 + 1, HC = BW / 2;
+  float2 col[BH];
+  if (c == 0) {
+#pragma unroll
+    for (int h = 0; h < BH; h++) {
+      const float2 x0 = Sb[h * NH], xn = Sb[h * NH + HC];
+      col[h] = make_float2(x0.x - xn.y, x0.y + xn.x);  // x0 + i xn
+    }
+    cfft<BH, +1>(col);
+#pragma unroll
+    for (int y = 0; y < BH; y++) {
+      Sb[y * NH] = make_float2(col[y].x, 0.f);
+      Sb[y * NH + HC] = make_float2(col[y].y, 0.f);
+    }
+  } else {
+#pragma unroll
+    for (int h = 0; h < BH; h++) col[h] = Sb[h * NH + c];
+    cfft<BH, +1>(col);
+#pragma unroll
+    for (int y = 0; y < BH; y++) Sb[y * NH + c] = col[y];
+  }
+}
+
+// Row y: c2r along x, written to out[0..BW) with 16-byte stores.
+template <int BW, int BH>
+__device__ __forceinline__ void inv_row(const float2* Sb, int y, float* out) {
+  constexpr int NH = BW / 2 + 1;
+  const float2* row = Sb + y * NH;
+  float2 c[NH];
+#pragma unroll
+  for (int k = 0; k < NH; k++) c[k] = row[k];
+  float r[BW];
+  irfft<BW>(c, r);
+  float4* o = reinterpret_cast<float4*>(out);
+#pragma unroll
+  for (int x = 0; x < BW / 4; x++) o[x] = make_float4(r[4 * x], r[4 * x + 1], r[4 * x + 2], r[4 * x + 3]);
+}
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // ---------------------------------------------------------------- forward
 
+// One warp transforms blocks_per_warp<BW>() consecutive blocks (rows, then
+// columns, then a coalesced 16-byte copy-out of the contiguous spectra).
 template <int BW, int BH, typename T>
 __global__ void __launch_bounds__(kWarps * 32) k_forward(ForwardArgs a) {
-  constexpr int NH = BW / 2 + 1, TP = BW + 1;
-  extern __shared__ float smem[];
+  constexpr int NH = BW / 2 + 1, HC = BW / 2, NBW = blocks_per_warp<BW>(), BINS = BH * NH;
+  extern __shared__ float2 smem2[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* tile = smem + warp * fft_smem_floats<BW, BH>();
-  float2* S = reinterpret_cast<float2*>(tile + BH * TP);
+  float2* S = smem2 + warp * NBW * BINS;
   const Geom& g = a.g;
-  const int blk = blockIdx.x * kWarps + warp;
-  if (blk >= g.nblocks) return;
-  const int by = blk / g.nox, bx = blk - by * g.nox;
-  // 1. windowed block tile (coalesced along x)
-  for (int y = 0; y < BH; y++) {
-    const int k = reflect101(by * g.sy + y - g.sy, g.H);
-    const T* srow = reinterpret_cast<const T*>(static_cast<const char*>(a.src) +
-                                               (long long)field_row(k, g.H, g.interlaced) * a.src_stride);
-    const float wy = __ldg(a.wan_y + y);
-    for (int x = lane; x < BW; x += 32) {
-      const int c = reflect101(bx * g.sx + x - g.sx, g.W);
-      const float v = load_sample<T>(srow + c) - a.base;
-      tile[y * TP + x] = v * __ldg(a.wan_x + x) * wy;
-    }
+  const int blk0 = (blockIdx.x * kWarps + warp) * NBW;
+  if (blk0 >= g.nblocks) return;
+  for (int t = lane; t < NBW * BH; t += 32) {
+    const int b = t / BH, y = t - b * BH;
+    if (blk0 + b < g.nblocks) fwd_row<BW, BH, T>(a, blk0 + b, y, S + b * BINS);
   }
   __syncwarp();
-  // 2. r2c along x, one row per lane
-  for (int y = lane; y < BH; y += 32) {
-    float r[BW];
-#pragma unroll
-    for (int x = 0; x < BW; x++) r[x] = tile[y * TP + x];
-    float2 c[NH];
-    rfft<BW>(r, c);
-#pragma unroll
-    for (int k = 0; k < NH; k++) S[y * NH + k] = c[k];
+  for (int t = lane; t < NBW * HC; t += 32) {
+    const int b = t / HC, c = t - b * HC;
+    if (blk0 + b < g.nblocks) fwd_col<BW, BH>(S + b * BINS, c);
   }
   __syncwarp();
-  // 3. complex DFT along y, one column per lane; rows of the output are
-  //    written by consecutive lanes (coalesced)
-  float2* out = a.spec + (size_t)blk * BH * NH;
-  for (int k = lane; k < NH; k += 32) {
-    float2 col[BH];
-#pragma unroll
-    for (int y = 0; y < BH; y++) col[y] = S[y * NH + k];
-    cfft<BH, -1>(col);
-#pragma unroll
-    for (int h = 0; h < BH; h++) out[h * NH + k] = col[h];
-  }
+  const int nvalid = min(NBW, g.nblocks - blk0);
+  float4* dst = reinterpret_cast<float4*>(a.spec + (size_t)blk0 * BINS);
+  const float4* src = reinterpret_cast<const float4*>(S);
+  for (int i = lane; i < nvalid * BINS / 2; i += 32) dst[i] = src[i];
 }
 
 // ---------------------------------------------------------------- filters
@@ -101,27 +224,30 @@ __global__ void __launch_bounds__(kWarps * 32) k_forward(ForwardArgs a) {
 __device__ __forceinline__ float sharpen_fact(const InverseArgs& a, float psd, int bin) {
   // src/code_impl/Apply.cpp:129-131
   return 1.f + a.c.sharpen * __ldg(a.t.wsharpen + bin) *
-                   sqrtf(psd * a.c.smax2n / ((psd + a.c.smin2n) * (psd + a.c.smax2n)));
+                   sqrtf(__fdividef(psd * a.c.smax2n, (psd + a.c.smin2n) * (psd + a.c.smax2n)));
 }
 __device__ __forceinline__ float dehalo_fact(const InverseArgs& a, float psd, int bin) {
   // src/code_impl/Apply.cpp:132
-  return (psd + a.c.ht2n) / ((psd + a.c.ht2n) + a.c.dehalo * __ldg(a.t.wdehalo + bin) * psd);
+  return __fdividef(psd + a.c.ht2n, (psd + a.c.ht2n) + a.c.dehalo * __ldg(a.t.wdehalo + bin) * psd);
 }
 
 // limited Wiener factor applied to one temporal component, code_impl_C.h:34-40
+// (divisions use the fast reciprocal: <= 2 ulp, far inside the +-1 LSB output bar)
 __device__ __forceinline__ void wiener(float& re, float& im, float noise, float lowlimit) {
   const float psd = re * re + im * im + 1.0e-15f;
-  const float q = (psd - noise) / psd;
+  const float q = __fdividef(psd - noise, psd);
   const float f = q > lowlimit ? q : lowlimit;
   re *= f;
   im *= f;
 }
 
-// Filtered value of one bin. MODE: 1 = Wiener 2D, 2..5 = Wiener 3D,
+// Filtered value of one bin from its values w[0..4] in frames n-2..n+2 (only
+// the window's entries are read). MODE: 1 = Wiener 2D, 2..5 = Wiener 3D,
 // 0 = Kalman (updates the state when `commit`), -1 = sharpen only (identity).
 template <int MODE>
-__device__ __forceinline__ float2 filter_bin(const InverseArgs& a, size_t off, int bin, float gf, bool commit) {
-  const float2 cur = a.in[2][off + bin];
+__device__ __forceinline__ float2 filter_vals(const InverseArgs& a, const float2 (&w)[5], size_t off, int bin, float gf,
+                                              bool commit) {
+  const float2 cur = w[2];
   if constexpr (MODE == MODE_SHARPEN_ONLY) {
     return cur;
   } else if constexpr (MODE == MODE_KALMAN) {
@@ -140,7 +266,7 @@ __device__ __forceinline__ float2 filter_bin(const InverseArgs& a, size_t off, i
       last = cur;
     } else {
       const float sum = cv + cp;
-      const float gain = sum / (sum + sigma);
+      const float gain = __fdividef(sum, sum + sigma);
       cp = gain * gain * sigma;
       cv = (1.f - gain) * sum;
       last.x = gain * cur.x + (1.f - gain) * last.x;
@@ -162,7 +288,7 @@ __device__ __forceinline__ float2 filter_bin(const InverseArgs& a, size_t off, i
     const float cr = cur.x - gc.x, ci = cur.y - gc.y;
     const float psd = cr * cr + ci * ci + 1e-15f;
     const float noise = a.c.pattern ? __ldg(a.t.pattern2d + bin) : a.c.sigma2n;
-    const float q = (psd - noise) / psd;
+    const float q = __fdividef(psd - noise, psd);
     float f = q > a.c.lowlimit ? q : a.c.lowlimit;
     if (a.c.fuse_sharpen) {
       if (a.c.use_sharpen && a.c.use_dehalo) f *= sharpen_fact(a, psd, bin) * dehalo_fact(a, psd, bin);
@@ -183,7 +309,7 @@ __device__ __forceinline__ float2 filter_bin(const InverseArgs& a, size_t off, i
     const float ll = a.c.lowlimit;
     const float cr = cur.x, ci = cur.y;
     if constexpr (MODE == 2) {
-      const float2 pv = a.in[1][off + bin];
+      const float2 pv = w[1];
       float f0r = cr + pv.x - g0, f0i = ci + pv.y - g1;
       float f1r = cr - pv.x, f1i = ci - pv.y;
       wiener(f0r, f0i, noise, ll);
@@ -191,7 +317,7 @@ __device__ __forceinline__ float2 filter_bin(const InverseArgs& a, size_t off, i
       return make_float2((f0r + f1r + g0) * 0.5f, (f0i + f1i + g1) * 0.5f);
     } else if constexpr (MODE == 3) {
       const float sin120 = 0.86602540378443864676372317075294f;
-      const float2 pv = a.in[1][off + bin], nx = a.in[3][off + bin];
+      const float2 pv = w[1], nx = w[3];
       const float pnr = pv.x + nx.x, pni = pv.y + nx.y;
       float fcr = cr + pnr - g0, fci = ci + pni - g1;
       const float di = sin120 * (pv.y - nx.y), dr = sin120 * (nx.x - pv.x);
@@ -203,7 +329,7 @@ __device__ __forceinline__ float2 filter_bin(const InverseArgs& a, size_t off, i
       const float third = 1.0f / 3.0f;
       return make_float2((fcr + fpr + fnr + g0) * third, (fci + fpi + fni + g1) * third);
     } else if constexpr (MODE == 4) {
-      const float2 p2 = a.in[0][off + bin], pv = a.in[1][off + bin], nx = a.in[3][off + bin];
+      const float2 p2 = w[0], pv = w[1], nx = w[3];
       float fp2r = (cr + p2.x) - (pv.x + nx.x), fp2i = (ci + p2.y) - (pv.y + nx.y);
       float fpr = (cr - p2.x) + (pv.y - nx.y), fpi = (ci - p2.y) - (pv.x - nx.x);
       float fcr = (cr + p2.x) + (pv.x + nx.x) - g0, fci = (ci + p2.y) + (pv.y + nx.y) - g1;
@@ -216,8 +342,8 @@ __device__ __forceinline__ float2 filter_bin(const InverseArgs& a, size_t off, i
     } else {
       const float sin72 = 0.95105651629515357211643933337938f, cos72 = 0.30901699437494742410229341718282f;
       const float sin144 = 0.58778525229247312916870595463907f, cos144 = -0.80901699437494742410229341718282f;
-      const float2 p2 = a.in[0][off + bin], pv = a.in[1][off + bin];
-      const float2 nx = a.in[3][off + bin], n2 = a.in[4][off + bin];
+      const float2 p2 = w[0], pv = w[1];
+      const float2 nx = w[3], n2 = w[4];
       float sum = (p2.x + n2.x) * cos72 + (pv.x + nx.x) * cos144 + cr;
       float dif = (-p2.y + n2.y) * sin72 + (pv.y - nx.y) * sin144;
       float fp2r = sum + dif, fn2r = sum - dif;
@@ -243,6 +369,22 @@ __device__ __forceinline__ float2 filter_bin(const InverseArgs& a, size_t off, i
   }
 }
 
+// Window slots 2 - MODE/2 .. 2 + (MODE-1)/2 of a MODE-frame Wiener 3D (the
+// reference's apply_in[] table, src/fft3d_engine.h:634-644); one slot otherwise.
+template <int MODE>
+__host__ __device__ constexpr int win_lo() { return MODE >= 2 ? 2 - MODE / 2 : 2; }
+template <int MODE>
+__host__ __device__ constexpr int win_hi() { return MODE >= 2 ? 2 + (MODE - 1) / 2 : 2; }
+
+template <int MODE>
+__device__ __forceinline__ float2 filter_bin(const InverseArgs& a, size_t off, int bin, float gf, bool commit) {
+  float2 w[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++)
+    w[k] = (k >= win_lo<MODE>() && k <= win_hi<MODE>()) ? __ldg(a.in[k] + off + bin) : make_float2(0.f, 0.f);
+  return filter_vals<MODE>(a, w, off, bin, gf, commit);
+}
+
 // separate sharpen/dehalo pass on a filtered bin, src/code_impl/Sharpen.cpp:13-63
 __device__ __forceinline__ float2 sharpen_bin(const InverseArgs& a, float2 v, int bin, float gf) {
   float2 gc = make_float2(0.f, 0.f);
@@ -261,61 +403,162 @@ __device__ __forceinline__ float2 sharpen_bin(const InverseArgs& a, float2 v, in
 
 // ---------------------------------------------------------------- inverse
 
+// One warp filters and inverse-transforms blocks_per_warp<BW>() blocks:
+//  A. every bin of a block, consecutive bins on consecutive lanes (coalesced
+//     loads of the bt spectra), through the filter and the separate
+//     sharpen/dehalo pass (whose grid fraction is the filtered DC, lane 0's
+//     first bin); results to shared memory;
+//  B. one column per lane: inverse complex DFT along y (DC and Nyquist columns
+//     together: both are Hermitian, so their inverses are real);
+//  C. one row per lane: c2r along x, 16-byte stores of the time-domain rows.
 template <int BW, int BH, int MODE>
 __global__ void __launch_bounds__(kWarps * 32) k_filter_inverse(InverseArgs a) {
-  constexpr int NH = BW / 2 + 1, TP = BW + 1;
-  extern __shared__ float smem[];
+  constexpr int NH = BW / 2 + 1, HC = BW / 2, NBW = blocks_per_warp<BW>(), BINS = BH * NH;
+  constexpr int PER = (BINS + 31) / 32;
+  extern __shared__ float2 smem2[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* tile = smem + warp * fft_smem_floats<BW, BH>();
-  float2* S = reinterpret_cast<float2*>(tile + BH * TP);
+  float2* S = smem2 + warp * NBW * BINS;
   const Geom& g = a.g;
-  const int blk = blockIdx.x * kWarps + warp;
-  if (blk >= g.nblocks) return;
-  const size_t off = (size_t)blk * BH * NH;
+  const int cta = a.reverse ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
+  const int blk0 = (cta * kWarps + warp) * NBW;
+  if (blk0 >= g.nblocks) return;
   const float gs0 = __ldg(&a.t.grid[0].x);
-  const float gf = (MODE >= 1) ? a.c.degrid * a.in[2][off].x / gs0 : 0.f;
-  // grid fraction of the separate sharpen pass: the DC of the FILTERED block
-  // (Sharpen.cpp reads its input spectrum), recomputed by every lane
-  float gf_sh = 0.f;
-  if (a.c.do_sharpen) gf_sh = a.c.degrid * filter_bin<MODE>(a, off, 0, gf, false).x / gs0;
-  // 1. filter every bin, then the inverse DFT along y (one column per lane)
-  for (int k = lane; k < NH; k += 32) {
-    float2 col[BH];
+  constexpr int LO = win_lo<MODE>(), NW = win_hi<MODE>() - win_lo<MODE>() + 1;
+  constexpr int D = PER < 4 ? PER : 4;  // load-pipeline depth (chunks of 32 bins in flight)
+#pragma unroll 1
+  for (int b = 0; b < NBW; b++) {
+    const int blk = blk0 + b;
+    if (blk >= g.nblocks) break;
+    const size_t off = (size_t)blk * BINS;
+    const float gf = (MODE >= 1) ? a.c.degrid * __ldg(&a.in[2][off].x) / gs0 : 0.f;
+    // software pipeline: the window's values of chunk j + D are loaded while
+    // chunk j is filtered, so D x NW loads per lane are always in flight
+    float2 buf[D][NW];
+    auto load = [&](int j, float2(&dst)[NW]) {
+      const int i = lane + 32 * j;
 #pragma unroll
-    for (int h = 0; h < BH; h++) {
-      const int bin = h * NH + k;
-      float2 v = filter_bin<MODE>(a, off, bin, gf, true);
-      if (a.c.do_sharpen) v = sharpen_bin(a, v, bin, gf_sh);
-      col[h] = v;
+      for (int k = 0; k < NW; k++) dst[k] = i < BINS ? __ldg(a.in[LO + k] + off + i) : make_float2(0.f, 0.f);
+    };
+#pragma unroll
+    for (int j = 0; j < D; j++) load(j, buf[j]);
+    float gsh = 0.f;
+#pragma unroll
+    for (int j = 0; j < PER; j++) {
+      const int i = lane + 32 * j;
+      float2 w[5];
+#pragma unroll
+      for (int k = 0; k < 5; k++) w[k] = (k >= LO && k < LO + NW) ? buf[j % D][k - LO] : make_float2(0.f, 0.f);
+      if (j + D < PER) load(j + D, buf[j % D]);
+      float2 v = make_float2(0.f, 0.f);
+      if (i < BINS) v = filter_vals<MODE>(a, w, off, i, gf, true);
+      if (a.c.do_sharpen) {
+        // grid fraction of the sharpen pass: the filtered DC (lane 0, chunk 0)
+        if (j == 0) gsh = a.c.degrid * __shfl_sync(0xffffffffu, v.x, 0) / gs0;
+        if (i < BINS) v = sharpen_bin(a, v, i, gsh);
+      }
+      if (i < BINS) S[b * BINS + i] = v;
     }
-    cfft<BH, +1>(col);
-#pragma unroll
-    for (int h = 0; h < BH; h++) S[h * NH + k] = col[h];
   }
   __syncwarp();
-  // 2. c2r along x, one row per lane
-  for (int y = lane; y < BH; y += 32) {
-    float2 c[NH];
-#pragma unroll
-    for (int k = 0; k < NH; k++) c[k] = S[y * NH + k];
-    float r[BW];
-    irfft<BW>(c, r);
-#pragma unroll
-    for (int x = 0; x < BW; x++) tile[y * TP + x] = r[x];
+  for (int t = lane; t < NBW * HC; t += 32) {
+    const int b = t / HC, c = t - b * HC;
+    if (blk0 + b < g.nblocks) inv_col<BW, BH>(S + b * BINS, c);
   }
   __syncwarp();
-  // 3. coalesced store of the time-domain block
-  float* out = a.tdom + (size_t)blk * BH * BW;
-  for (int y = 0; y < BH; y++)
-    for (int x = lane; x < BW; x += 32) out[y * BW + x] = tile[y * TP + x];
+  for (int t = lane; t < NBW * BH; t += 32) {
+    const int b = t / BH, y = t - b * BH, blk = blk0 + b;
+    if (blk < g.nblocks) inv_row<BW, BH>(S + b * BINS, y, a.tdom + ((size_t)blk * BH + y) * BW);
+  }
+}
+
+// ---------------------------------------------------------------- fused
+
+// Steady-state hot path of one output frame: one warp per block
+//  0. cp.async copies of the older frames' spectra of the block into shared
+//     memory (they land while step 1 computes);
+//  1. forward transform of the window's newest frame (rows, columns) and its
+//     spectrum stored to the ring for the next output frames;
+//  2. filter of every bin (lane-consecutive bins), separate sharpen/dehalo pass;
+//  3. inverse transform (columns, rows) to the time-domain blocks.
+template <int BW, int BH, typename T, int MODE>
+__global__ void __launch_bounds__(kFusedWarps * 32) k_fused(FusedArgs A) {
+  constexpr int NH = BW / 2 + 1, HC = BW / 2, BINS = BH * NH, PER = (BINS + 31) / 32;
+  constexpr int LO = win_lo<MODE>(), HI = win_hi<MODE>(), NOLD = HI - LO;
+  const InverseArgs& a = A.v;
+  const Geom& g = a.g;
+  extern __shared__ float2 smem2[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* S = smem2 + warp * BINS * (1 + NOLD);
+  float2* old = S + BINS;
+  const int cta = a.reverse ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
+  const int blk = cta * kFusedWarps + warp;
+  if (blk >= g.nblocks) return;
+  const size_t off = (size_t)blk * BINS;
+#pragma unroll
+  for (int q = 0; q < NOLD; q++) {
+    const float4* src = reinterpret_cast<const float4*>(a.in[LO + q] + off);
+    float4* dst = reinterpret_cast<float4*>(old + q * BINS);
+    for (int i = lane; i < BINS / 2; i += 32) cp_async16(dst + i, src + i);
+  }
+  cp_async_commit();
+  for (int y = lane; y < BH; y += 32) fwd_row<BW, BH, T>(A.f, blk, y, S);
+  __syncwarp();
+  for (int c = lane; c < HC; c += 32) fwd_col<BW, BH>(S, c);
+  __syncwarp();
+  {
+    float4* dst = reinterpret_cast<float4*>(A.f.spec + off);
+    const float4* src = reinterpret_cast<const float4*>(S);
+    for (int i = lane; i < BINS / 2; i += 32) dst[i] = src[i];
+  }
+  cp_async_wait_all();
+  __syncwarp();
+  const float gs0 = __ldg(&a.t.grid[0].x);
+  float gf = 0.f;
+  if constexpr (MODE >= 1) gf = a.c.degrid * (HI == 2 ? S[0].x : old[(2 - LO) * BINS].x) / gs0;
+  __syncwarp();  // every lane has read the DC before lane 0 rewrites it
+  float2 v[PER];
+#pragma unroll
+  for (int j = 0; j < PER; j++) {
+    const int i = lane + 32 * j;
+    if (i < BINS) {
+      float2 w[5];
+#pragma unroll
+      for (int k = 0; k < 5; k++)
+        w[k] = (k == HI) ? S[i] : ((k >= LO && k < HI) ? old[(k - LO) * BINS + i] : make_float2(0.f, 0.f));
+      v[j] = filter_vals<MODE>(a, w, off, i, gf, true);
+    }
+  }
+  if (a.c.do_sharpen) {
+    const float gsh = a.c.degrid * __shfl_sync(0xffffffffu, v[0].x, 0) / gs0;
+#pragma unroll
+    for (int j = 0; j < PER; j++) {
+      const int i = lane + 32 * j;
+      if (i < BINS) v[j] = sharpen_bin(a, v[j], i, gsh);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < PER; j++) {
+    const int i = lane + 32 * j;
+    if (i < BINS) S[i] = v[j];
+  }
+  __syncwarp();
+  for (int c = lane; c < HC; c += 32) inv_col<BW, BH>(S, c);
+  __syncwarp();
+  for (int y = lane; y < BH; y += 32) inv_row<BW, BH>(S, y, a.tdom + ((size_t)blk * BH + y) * BW);
 }
 
 // ---------------------------------------------------------------- launchers
 
 template <int BW, int BH>
+int fft_grid(int nblocks) {
+  const int per_cta = kWarps * blocks_per_warp<BW>();
+  return (nblocks + per_cta - 1) / per_cta;
+}
+
+template <int BW, int BH>
 cudaError_t fwd_sized(const ForwardArgs& a, int bytes, cudaStream_t s) {
-  const int smem = kWarps * fft_smem_floats<BW, BH>() * 4;
-  const int grid = (a.g.nblocks + kWarps - 1) / kWarps;
+  const int smem = kWarps * fft_smem_bytes<BW, BH>();
+  const int grid = fft_grid<BW, BH>(a.g.nblocks);
   cudaError_t e = cudaSuccess;
   if (bytes == 1) {
     e = cudaFuncSetAttribute(k_forward<BW, BH, uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -332,13 +575,46 @@ cudaError_t fwd_sized(const ForwardArgs& a, int bytes, cudaStream_t s) {
 
 template <int BW, int BH, int MODE>
 cudaError_t inv_mode(const InverseArgs& a, cudaStream_t s) {
-  const int smem = kWarps * fft_smem_floats<BW, BH>() * 4;
-  const int grid = (a.g.nblocks + kWarps - 1) / kWarps;
+  const int smem = kWarps * fft_smem_bytes<BW, BH>();
+  const int grid = fft_grid<BW, BH>(a.g.nblocks);
   cudaError_t e =
       cudaFuncSetAttribute(k_filter_inverse<BW, BH, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
   k_filter_inverse<BW, BH, MODE><<<grid, kWarps * 32, smem, s>>>(a);
   return cudaGetLastError();
+}
+
+template <int BW, int BH, typename T, int MODE>
+cudaError_t fused_mode(const FusedArgs& a, cudaStream_t s) {
+  constexpr int NOLD = win_hi<MODE>() - win_lo<MODE>();
+  const int smem = kFusedWarps * BH * (BW / 2 + 1) * 8 * (1 + NOLD);
+  const int grid = (a.v.g.nblocks + kFusedWarps - 1) / kFusedWarps;
+  cudaError_t e =
+      cudaFuncSetAttribute(k_fused<BW, BH, T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  k_fused<BW, BH, T, MODE><<<grid, kFusedWarps * 32, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int BW, int BH, typename T>
+cudaError_t fused_typed(const FusedArgs& a, int mode, cudaStream_t s) {
+  switch (mode) {
+    case MODE_SHARPEN_ONLY: return fused_mode<BW, BH, T, MODE_SHARPEN_ONLY>(a, s);
+    case MODE_KALMAN: return fused_mode<BW, BH, T, MODE_KALMAN>(a, s);
+    case 1: return fused_mode<BW, BH, T, 1>(a, s);
+    case 2: return fused_mode<BW, BH, T, 2>(a, s);
+    case 3: return fused_mode<BW, BH, T, 3>(a, s);
+    case 4: return fused_mode<BW, BH, T, 4>(a, s);
+    case 5: return fused_mode<BW, BH, T, 5>(a, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <int BW, int BH>
+cudaError_t fused_sized(const FusedArgs& a, int mode, int bytes, cudaStream_t s) {
+  if (bytes == 1) return fused_typed<BW, BH, uint8_t>(a, mode, s);
+  if (bytes == 2) return fused_typed<BW, BH, uint16_t>(a, mode, s);
+  return cudaErrorNotSupported;  // float samples use the unfused path
 }
 
 template <int BW, int BH>
@@ -360,6 +636,6 @@ cudaError_t inv_sized(const InverseArgs& a, int mode, cudaStream_t s) {
 // Registers block size BW x BH of this translation unit in the size table.
 #define FFT3D_REGISTER_SIZE(BW, BH)                                                                  \
   static const bool fft3d_reg_##BW##x##BH = register_size(                                          \
-      SizeEntry{BW, BH, &fwd_sized<BW, BH>, &inv_sized<BW, BH>, &upload_twiddle_table});
+      SizeEntry{BW, BH, &fwd_sized<BW, BH>, &inv_sized<BW, BH>, &fused_sized<BW, BH>, &upload_twiddle_table});
 
 }  // namespace fft3d

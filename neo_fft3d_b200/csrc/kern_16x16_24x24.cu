@@ -1,0 +1,7 @@
+// Kernel instantiations for block sizes (bw x bh): 16 16, 24 24.
+#include "fft3d_kernels_impl.cuh"
+
+namespace fft3d {
+FFT3D_REGISTER_SIZE(16, 16)
+FFT3D_REGISTER_SIZE(24, 24)
+}  // namespace fft3d

@@ -12,6 +12,7 @@ struct SizeEntry {
   int bw, bh;
   cudaError_t (*fwd)(const ForwardArgs&, int bytes_per_sample, cudaStream_t);
   cudaError_t (*inv)(const InverseArgs&, int mode, cudaStream_t);
+  cudaError_t (*fused)(const FusedArgs&, int mode, int bytes_per_sample, cudaStream_t);
   cudaError_t (*upload)();  // the translation unit's twiddle table, once per device
 };
 
