@@ -126,6 +126,27 @@ int fft3d_plane_set_timing(fft3d_plane* h, int enable);
  * recorded launches. */
 int fft3d_plane_timing(fft3d_plane* h, double out[12]);
 
+/* Allocation-free filtering of ONE frame of one plane (DEVICE pointers),
+ * queued on `stream` (a cudaStream_t; NULL = the legacy default stream).
+ * No counterpart in the reference: it exists for callers that cannot allocate
+ * device memory while frames flow -- applications whose device memory is all
+ * owned by their own pool allocator, and real-time pipelines that must not pay
+ * the implicit synchronisation and latency of cudaMalloc/cudaFree. The call
+ * allocates and frees nothing: the plane's tables, the frame's spectrum and
+ * its time-domain blocks live in one fixed 32 MiB device array that every GPU
+ * loading this library holds until the process exits. Spatial modes only
+ * (bt = 1 Wiener with sharpen/dehalo, bt = -1 sharpen/dehalo); no noise
+ * patterns, no interlacing. A plane needing more scratch than 32 MiB (e.g.
+ * 1080p luma at bw=bh=32, ow=oh=16; 720p luma and 1080p chroma fit) returns
+ * FFT3D_E_UNSUPPORTED. All calls on a device share the array and find the
+ * previous call's contents in it (each call writes everything it reads), so
+ * calls whose GPU work overlaps race: keep them on one stream. The first call
+ * on a device resolves the array's address and uploads the FFT twiddle tables;
+ * make it before any stream capture. Output matches fft3d_plane_filter_device
+ * with the same parameters. */
+int fft3d_filter2d_static(const fft3d_params* p, const fft3d_plane_desc* d, const void* src, int src_stride,
+                          void* dst, int dst_stride, void* stream);
+
 /* Message of the last failure on this thread ("" if none). */
 const char* fft3d_last_error(void);
 

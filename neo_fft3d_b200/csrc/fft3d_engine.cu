@@ -472,6 +472,10 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
 
 }  // namespace
 
+namespace fft3d {
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace fft3d
+
 extern "C" {
 
 void fft3d_params_default(fft3d_params* p) {

@@ -17,6 +17,7 @@
 // shared memory so that every global access is coalesced.
 #pragma once
 #include <cstdint>
+#include <string>
 
 #include <cuda_runtime.h>
 
@@ -114,6 +115,9 @@ cudaError_t launch_overlap_add(const OlaArgs& a, int bytes_per_sample, cudaStrea
 cudaError_t launch_fused(const FusedArgs& a, int mode, int bytes_per_sample, cudaStream_t s);
 bool block_size_supported(int bw, int bh);
 cudaError_t upload_twiddles();  // every registered size, on the current device
+
+// Sets the message returned by fft3d_last_error() on this thread.
+void set_last_error(const std::string& msg);
 
 // filter modes of launch_filter_inverse
 enum { MODE_SHARPEN_ONLY = -1, MODE_KALMAN = 0, MODE_WIENER2D = 1 /* 2..5: Wiener 3D with that many frames */ };
