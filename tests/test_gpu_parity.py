@@ -74,8 +74,8 @@ def _oracle_pattern(planes, **case):
                                   dict(sigma=3.0, bt=3)], ids=["kalman48", "wiener3"])
 def test_clip_parity_10bit(gpu, case):
     planes = synth.make_clip(176, 144, 6, bits=10, noise_sigma=12, seed=12)
-    want = restate.filter_clip(planes, **case)
-    got = engine.filter_clip(planes, **case)
+    want = restate.filter_clip(planes, bits=10, **case)
+    got = engine.filter_clip(planes, bits=10, **case)
     for g, w in zip(got, want):
         mx, frac = _compare(g, w)
         assert frac >= PIX_TOL_FRAC, (case, mx, frac)
