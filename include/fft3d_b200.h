@@ -122,9 +122,10 @@ int fft3d_plane_set_timing(fft3d_plane* h, int enable);
  * interface must read and write once), for k = 0 forward (gather + window +
  * r2c), 1 filter + inverse (spectra in, time-domain blocks out), 2 overlap-add
  * (time-domain blocks in, pixels out), 3 fused (newest frame's pixels and the
- * older spectra in; newest spectrum and time-domain blocks out). Waits for the
+ * older spectra in; newest spectrum and time-domain blocks out), 4 streaming
+ * filter (the window's spectra in, filtered spectrum out). Waits for the
  * recorded launches. */
-int fft3d_plane_timing(fft3d_plane* h, double out[12]);
+int fft3d_plane_timing(fft3d_plane* h, double out[15]);
 
 /* Allocation-free filtering of ONE frame of one plane (DEVICE pointers),
  * queued on `stream` (a cudaStream_t; NULL = the legacy default stream).

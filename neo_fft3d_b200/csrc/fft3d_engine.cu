@@ -50,7 +50,7 @@ struct Slot {
 
 // Optional per-kernel timing: CUDA events recorded on the launching stream
 // around every launch, resolved when the counters are read.
-enum { K_FORWARD = 0, K_INVERSE = 1, K_OLA = 2, K_FUSED = 3, K_COUNT = 4 };
+enum { K_FORWARD = 0, K_INVERSE = 1, K_OLA = 2, K_FUSED = 3, K_FILTER = 4, K_COUNT = 5 };
 struct Timed {
   int kind;
   double bytes;
@@ -89,9 +89,13 @@ struct fft3d_plane {
   void* d_out = nullptr;  // staging of the host output (whole plane)
   size_t out_pitch = 0;
   uint64_t frames_done = 0;
-  // steady-state kernel choice: k_fused (forward + filter + inverse in one
-  // launch) or k_forward then k_filter_inverse; NEO_FFT3D_FUSED=1 selects fused
-  bool fused = false;
+  // kernel sequence of one output frame (NEO_FFT3D_PATH = unfused (default) | split | fused):
+  //   split:   k_forward (new frame), k_filter_bins (streaming filter of all
+  //            bins into d_filt), k_filter_inverse<sharpen only> on d_filt
+  //   unfused: k_forward, k_filter_inverse (filter + sharpen + inverse)
+  //   fused:   k_fused (new frame's forward + filter + inverse in one launch)
+  int path = 1;  // 0 split, 1 unfused, 2 fused
+  float2* d_filt = nullptr;
   bool timing = false;
   std::vector<Timed> pending;
   std::vector<cudaEvent_t> event_pool;
@@ -239,6 +243,7 @@ void free_plane(fft3d_plane* P) {
   for (auto& s : P->slots) cudaFree(s.spec);
   cudaFree(P->d_tables);
   cudaFree(P->d_tdom);
+  cudaFree(P->d_filt);
   cudaFree(P->d_last);
   cudaFree(P->d_cov);
   cudaFree(P->d_covp);
@@ -353,7 +358,7 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
   // of the window, in the fused kernel; older frames missing from the ring
   // (clip start, seeks) are transformed first by the forward kernel.
   const int newest = n + to;
-  const bool fused = P->fused && P->bytes != 4 && !find_slot(P, newest);
+  const bool fused = P->path == 2 && P->bytes != 4 && !find_slot(P, newest);
   for (int d = from; d <= (fused ? to - 1 : to); d++) {
     Slot* s = nullptr;
     int rc = spectrum_slot(P, n + d, n + from, n + to, src ? src[2 + d] : nullptr, stride ? stride[2 + d] : 0, host,
@@ -415,6 +420,19 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
       fa.v = ia;
       TimeScope ts(P, K_FUSED, (double)P->g.W * P->g.H * P->bytes + (to - from) * S + S + state + T, st);
       CK(fft3d::launch_fused(fa, mode, P->bytes, st), "fused kernel");
+    } else if (P->path == 0 && mode != fft3d::MODE_SHARPEN_ONLY) {
+      {
+        // reads: the spectra of the window (+ Kalman state); writes: the filtered spectrum
+        TimeScope ts(P, K_FILTER, (to - from + 1) * S + state + S, st);
+        CK(fft3d::launch_filter_bins(ia, P->d_filt, mode, st), "filter kernel");
+      }
+      g_launches++;
+      fft3d::InverseArgs sa = ia;
+      for (auto& p : sa.in) p = nullptr;
+      sa.in[2] = P->d_filt;
+      // reads: the filtered spectrum; writes: the time-domain blocks
+      TimeScope ts(P, K_INVERSE, S + T, st);
+      CK(fft3d::launch_filter_inverse(sa, fft3d::MODE_SHARPEN_ONLY, st), "sharpen/inverse kernel");
     } else {
       // reads: the spectra of the window (+ Kalman state); writes: the time-domain blocks
       TimeScope ts(P, K_INVERSE, (to - from + 1) * S + state + T, st);
@@ -504,8 +522,9 @@ int fft3d_plane_create(const fft3d_params* p, const fft3d_plane_desc* d, int dev
   P->d = *d;
   P->device = device;
   {
-    const char* f = std::getenv("NEO_FFT3D_FUSED");
-    P->fused = f && f[0] == '1';
+    const char* f = std::getenv("NEO_FFT3D_PATH");
+    std::string v = f ? f : "unfused";
+    P->path = v == "fused" ? 2 : (v == "split" ? 0 : 1);
   }
   fft3d_params& ep = P->ep;
   if (d->bits < 8 || (d->bits > 16 && d->bits != 32)) { delete P; return fail(FFT3D_E_PARAM, "neo_fft3d: unsupported bit depth"); }
@@ -654,6 +673,8 @@ int fft3d_plane_create(const fft3d_params* p, const fft3d_plane_desc* d, int dev
     if (cudaMalloc(&s.spec, P->spec_elems() * sizeof(float2)) != cudaSuccess)
       return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (spectrum ring)"));
   }
+  if (P->path == 0 && cudaMalloc(&P->d_filt, P->spec_elems() * sizeof(float2)) != cudaSuccess)
+    return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (filtered spectrum)"));
   if (cudaMalloc(&P->d_tdom, (size_t)g.nblocks * bh * bw * sizeof(float)) != cudaSuccess)
     return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (time-domain blocks)"));
   if (ep.bt == 0) {  // Kalman state, :339-344
@@ -762,7 +783,7 @@ int fft3d_plane_set_timing(fft3d_plane* P, int enable) {
   return FFT3D_OK;
 }
 
-int fft3d_plane_timing(fft3d_plane* P, double out[12]) {
+int fft3d_plane_timing(fft3d_plane* P, double out[15]) {
   if (!P || !out) return fail(FFT3D_E_PARAM, "neo_fft3d: null argument");
   std::lock_guard<std::mutex> lk(P->mu);
   CK(cudaSetDevice(P->device), "cudaSetDevice");

@@ -1,9 +1,11 @@
 // Size table, overlap-add kernel and launch dispatch of the FFT3D filtering
 // core; the FFT kernels themselves are instantiated in kern_*.cu.
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
 #include "fft3d_kernels.cuh"
+#include "fft3d_kernels_impl.cuh"
 #include "kern_registry.h"
 
 namespace fft3d {
@@ -13,14 +15,6 @@ namespace {
 std::vector<SizeEntry>& table() {
   static std::vector<SizeEntry> t;
   return t;
-}
-
-// processed-plane row k -> destination row (interlaced: field 1 first, then
-// field 2 bottom-up, src/buffer.cpp:99-115)
-__device__ __forceinline__ int field_row(int k, int H, int interlaced) {
-  if (!interlaced) return k;
-  int half = H >> 1;
-  return k < half ? 2 * k : H - 1 - 2 * (k - half);
 }
 
 template <typename T>
@@ -121,6 +115,25 @@ cudaError_t launch_forward(const ForwardArgs& a, int bytes, cudaStream_t s) {
 cudaError_t launch_filter_inverse(const InverseArgs& a, int mode, cudaStream_t s) {
   const SizeEntry* e = find_size(a.g.bw, a.g.bh);
   return e ? e->inv(a, mode, s) : cudaErrorInvalidValue;
+}
+
+cudaError_t launch_filter_bins(const InverseArgs& a, float2* F, int mode, cudaStream_t s) {
+  const int bins = a.g.bh * a.g.nh;
+  const size_t pairs = (size_t)a.g.nblocks * bins / 2;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = (int)std::min<size_t>((pairs + 255) / 256, (size_t)sms * 8);
+  switch (mode) {
+    case MODE_KALMAN: k_filter_bins<MODE_KALMAN><<<grid, 256, 0, s>>>(a, F, bins); break;
+    case 1: k_filter_bins<1><<<grid, 256, 0, s>>>(a, F, bins); break;
+    case 2: k_filter_bins<2><<<grid, 256, 0, s>>>(a, F, bins); break;
+    case 3: k_filter_bins<3><<<grid, 256, 0, s>>>(a, F, bins); break;
+    case 4: k_filter_bins<4><<<grid, 256, 0, s>>>(a, F, bins); break;
+    case 5: k_filter_bins<5><<<grid, 256, 0, s>>>(a, F, bins); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
 }
 
 cudaError_t launch_fused(const FusedArgs& a, int mode, int bytes, cudaStream_t s) {

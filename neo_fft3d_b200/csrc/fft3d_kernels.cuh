@@ -111,6 +111,9 @@ struct OlaArgs {
 cudaError_t launch_forward(const ForwardArgs& a, int bytes_per_sample, cudaStream_t s);
 cudaError_t launch_filter_inverse(const InverseArgs& a, int mode, cudaStream_t s);
 cudaError_t launch_overlap_add(const OlaArgs& a, int bytes_per_sample, cudaStream_t s);
+// Streaming filter of all bins (Wiener 2D/3D, Kalman) into F; the sharpen pass
+// and the inverse follow with launch_filter_inverse(MODE_SHARPEN_ONLY) on F.
+cudaError_t launch_filter_bins(const InverseArgs& a, float2* F, int mode, cudaStream_t s);
 // cudaErrorNotSupported when no fused kernel exists for the sample type (float)
 cudaError_t launch_fused(const FusedArgs& a, int mode, int bytes_per_sample, cudaStream_t s);
 bool block_size_supported(int bw, int bh);

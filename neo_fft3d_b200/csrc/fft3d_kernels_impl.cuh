@@ -168,19 +168,31 @@ __device__ __forceinline__ void inv_col(float2* Sb, int c) {
   }
 }
 
-// Row y: c2r along x, written to out[0..BW) with 16-byte stores.
+// Row y: c2r along x; the BW real samples overwrite the row's own storage in
+// Sb (BW floats fit in the row's BW/2+1 complex), for a coalesced copy-out.
 template <int BW, int BH>
-__device__ __forceinline__ void inv_row(const float2* Sb, int y, float* out) {
+__device__ __forceinline__ void inv_row_inplace(float2* Sb, int y) {
   constexpr int NH = BW / 2 + 1;
-  const float2* row = Sb + y * NH;
+  float2* row = Sb + y * NH;
   float2 c[NH];
 #pragma unroll
   for (int k = 0; k < NH; k++) c[k] = row[k];
   float r[BW];
   irfft<BW>(c, r);
-  float4* o = reinterpret_cast<float4*>(out);
 #pragma unroll
-  for (int x = 0; x < BW / 4; x++) o[x] = make_float4(r[4 * x], r[4 * x + 1], r[4 * x + 2], r[4 * x + 3]);
+  for (int x = 0; x < BW / 2; x++) row[x] = make_float2(r[2 * x], r[2 * x + 1]);
+}
+
+// Coalesced store of one block's time-domain rows (left in Sb by
+// inv_row_inplace, row pitch NH complex) to out[BH][BW].
+template <int BW, int BH>
+__device__ __forceinline__ void store_tdom(const float2* Sb, float* out, int lane) {
+  constexpr int NH = BW / 2 + 1, HALF = BW / 2;
+  float2* o = reinterpret_cast<float2*>(out);
+  for (int i = lane; i < BH * HALF; i += 32) {
+    const int y = i / HALF, x = i - y * HALF;
+    o[i] = Sb[y * NH + x];
+  }
 }
 
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
@@ -401,6 +413,40 @@ __device__ __forceinline__ float2 sharpen_bin(const InverseArgs& a, float2 v, in
   return make_float2(cr * f + gc.x, ci * f + gc.y);
 }
 
+// ---------------------------------------------------------------- filter (streaming)
+
+// Filter of every bin of every block as a flat stream: each thread takes two
+// neighbouring bins (one 16-byte load per window frame, one 16-byte store of
+// the filtered pair to F). No shared memory and few registers, so the SMs
+// hold enough warps to keep the spectrum reads at HBM speed. The separate
+// sharpen/dehalo pass, which needs each block's filtered DC, runs afterwards
+// in k_filter_inverse<MODE_SHARPEN_ONLY> on F.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_filter_bins(InverseArgs a, float2* F, int bins_per_block) {
+  constexpr int LO = win_lo<MODE>(), NW = win_hi<MODE>() - win_lo<MODE>() + 1;
+  const size_t pairs = (size_t)a.g.nblocks * bins_per_block / 2;
+  const float gs0 = __ldg(&a.t.grid[0].x);
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < pairs; q += (size_t)gridDim.x * blockDim.x) {
+    const size_t e = 2 * q;
+    const int bin = (int)(e % bins_per_block);
+    const size_t off = e - bin;
+    float4 wv[NW];
+#pragma unroll
+    for (int k = 0; k < NW; k++) wv[k] = __ldg(reinterpret_cast<const float4*>(a.in[LO + k] + e));
+    const float gf = (MODE >= 1) ? a.c.degrid * __ldg(&a.in[2][off].x) / gs0 : 0.f;
+    float2 w0[5], w1[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+      const bool in = k >= LO && k < LO + NW;
+      w0[k] = in ? make_float2(wv[k - LO].x, wv[k - LO].y) : make_float2(0.f, 0.f);
+      w1[k] = in ? make_float2(wv[k - LO].z, wv[k - LO].w) : make_float2(0.f, 0.f);
+    }
+    const float2 v0 = filter_vals<MODE>(a, w0, off, bin, gf, true);
+    const float2 v1 = filter_vals<MODE>(a, w1, off, bin + 1, gf, true);
+    reinterpret_cast<float4*>(F)[q] = make_float4(v0.x, v0.y, v1.x, v1.y);
+  }
+}
+
 // ---------------------------------------------------------------- inverse
 
 // One warp filters and inverse-transforms blocks_per_warp<BW>() blocks:
@@ -424,7 +470,10 @@ __global__ void __launch_bounds__(kWarps * 32) k_filter_inverse(InverseArgs a) {
   if (blk0 >= g.nblocks) return;
   const float gs0 = __ldg(&a.t.grid[0].x);
   constexpr int LO = win_lo<MODE>(), NW = win_hi<MODE>() - win_lo<MODE>() + 1;
-  constexpr int D = PER < 4 ? PER : 4;  // load-pipeline depth (chunks of 32 bins in flight)
+  // load-pipeline depth (chunks of 32 bins in flight): all chunks for a
+  // one-frame window, fewer as the window (and the registers per chunk) grows
+  constexpr int DW = NW == 1 ? PER : (NW == 2 ? 10 : (NW == 3 ? 7 : (NW == 4 ? 5 : 4)));
+  constexpr int D = PER < DW ? PER : DW;
 #pragma unroll 1
   for (int b = 0; b < NBW; b++) {
     const int blk = blk0 + b;
@@ -466,9 +515,12 @@ __global__ void __launch_bounds__(kWarps * 32) k_filter_inverse(InverseArgs a) {
   }
   __syncwarp();
   for (int t = lane; t < NBW * BH; t += 32) {
-    const int b = t / BH, y = t - b * BH, blk = blk0 + b;
-    if (blk < g.nblocks) inv_row<BW, BH>(S + b * BINS, y, a.tdom + ((size_t)blk * BH + y) * BW);
+    const int b = t / BH, y = t - b * BH;
+    if (blk0 + b < g.nblocks) inv_row_inplace<BW, BH>(S + b * BINS, y);
   }
+  __syncwarp();
+  for (int b = 0; b < NBW && blk0 + b < g.nblocks; b++)
+    store_tdom<BW, BH>(S + b * BINS, a.tdom + (size_t)(blk0 + b) * BH * BW, lane);
 }
 
 // ---------------------------------------------------------------- fused
@@ -544,7 +596,9 @@ __global__ void __launch_bounds__(kFusedWarps * 32) k_fused(FusedArgs A) {
   __syncwarp();
   for (int c = lane; c < HC; c += 32) inv_col<BW, BH>(S, c);
   __syncwarp();
-  for (int y = lane; y < BH; y += 32) inv_row<BW, BH>(S, y, a.tdom + ((size_t)blk * BH + y) * BW);
+  for (int y = lane; y < BH; y += 32) inv_row_inplace<BW, BH>(S, y);
+  __syncwarp();
+  store_tdom<BW, BH>(S, a.tdom + (size_t)blk * BH * BW, lane);
 }
 
 // ---------------------------------------------------------------- launchers

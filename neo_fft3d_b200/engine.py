@@ -21,7 +21,7 @@ SYMBOLS = ("fft3d_params_default", "fft3d_plane_create", "fft3d_plane_filter", "
            "fft3d_plane_cached", "fft3d_plane_spectrum", "fft3d_plane_geometry", "fft3d_plane_set_pattern_frame",
            "fft3d_plane_reset", "fft3d_plane_destroy", "fft3d_last_error", "fft3d_kernel_launches",
            "fft3d_plane_set_timing", "fft3d_plane_timing")
-KERNELS = ("forward", "filter_inverse", "overlap_add", "fused")
+KERNELS = ("forward", "filter_inverse", "overlap_add", "fused", "filter_bins")
 
 
 class FFT3DError(RuntimeError):
@@ -115,7 +115,7 @@ class PlaneEngine:
 
     def timing(self) -> dict:
         """{kernel: (launches, milliseconds, algorithmic bytes)}; resets the counters."""
-        out = (ctypes.c_double * 12)()
+        out = (ctypes.c_double * 15)()
         _check(lib().fft3d_plane_timing(self.h, out))
         return {k: (out[3 * i], out[3 * i + 1], out[3 * i + 2]) for i, k in enumerate(KERNELS)}
 
