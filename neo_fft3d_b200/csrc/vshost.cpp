@@ -329,7 +329,11 @@ const VSFrameRef* render(const std::shared_ptr<Node>& node, int n, std::string& 
 
 const VSFrameRef* VS_CC getFrameFilter(int n, VSNodeRef* node, VSFrameContext* ctx) noexcept {
   auto it = ctx->ready.find({node->node.get(), n});
-  return it == ctx->ready.end() ? nullptr : cloneFrameRef(it->second);
+  if (it != ctx->ready.end()) return cloneFrameRef(it->second);
+  // a frame the filter did not request: rendered on demand (VapourSynth
+  // itself would return NULL here)
+  std::string err;
+  return render(node->node, n, err);
 }
 void VS_CC requestFrameFilter(int n, VSNodeRef* node, VSFrameContext* ctx) noexcept {
   ctx->requests.emplace_back(node->node, n);

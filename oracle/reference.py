@@ -32,10 +32,10 @@ def core():
     return _core
 
 
-def run(planes, threads: int = 1, first: int = 0, count=None, bits=None, **kw):
+def run(clip_planes, threads: int = 1, first: int = 0, count=None, bits=None, **kw):
     """core.neo_fft3d.FFT3D(clip, **kw) rendered over frames [first, first+count).
     ``bits``: bit depth of uint16 planes (default 16)."""
     c = core()
-    clip = c.clip(planes, bits=bits)
+    clip = c.clip(clip_planes, bits=bits)
     out = c.invoke("neo_fft3d", "FFT3D", clip, **kw)
     return out.render(first=first, count=count, threads=threads)
