@@ -94,7 +94,11 @@ struct fft3d_plane {
   //            bins into d_filt), k_filter_inverse<sharpen only> on d_filt
   //   unfused: k_forward, k_filter_inverse (filter + sharpen + inverse)
   //   fused:   k_fused (new frame's forward + filter + inverse in one launch)
-  int path = 1;  // 0 split, 1 unfused, 2 fused
+  //   tc:      as unfused, with the forward transform on the tensor cores
+  //            (k_forward_tc, 32x32 blocks; other sizes fall back to k_forward)
+  int path = 1;  // 0 split, 1 unfused, 2 fused, 3 tc
+  uint8_t* d_tc = nullptr;  // tensor-core DFT tables (path 3)
+  int* d_err = nullptr;     // device error flag of the tensor-core kernels
   float2* d_filt = nullptr;
   bool timing = false;
   std::vector<Timed> pending;
@@ -244,6 +248,8 @@ void free_plane(fft3d_plane* P) {
   cudaFree(P->d_tables);
   cudaFree(P->d_tdom);
   cudaFree(P->d_filt);
+  cudaFree(P->d_tc);
+  cudaFree(P->d_err);
   cudaFree(P->d_last);
   cudaFree(P->d_cov);
   cudaFree(P->d_covp);
@@ -289,7 +295,11 @@ fft3d::ForwardArgs forward_args(fft3d_plane* P, const void* plane, long long str
 int launch_forward(fft3d_plane* P, const void* plane, long long stride, float2* spec, cudaStream_t st) {
   fft3d::ForwardArgs a = forward_args(P, plane, stride, spec);
   TimeScope ts(P, K_FORWARD, (double)P->g.W * P->g.H * P->bytes + (double)P->spec_elems() * sizeof(float2), st);
-  CK(fft3d::launch_forward(a, P->bytes, st), "forward kernel");
+  if (P->d_tc) {
+    CK(fft3d::launch_forward_tc(a, P->d_tc, P->d_err, P->bytes, st), "tensor-core forward kernel");
+  } else {
+    CK(fft3d::launch_forward(a, P->bytes, st), "forward kernel");
+  }
   g_launches++;
   return FFT3D_OK;
 }
@@ -484,6 +494,11 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
     CK(cudaMemcpy2DAsync(hdst, dst_stride, ddst, P->out_pitch, (size_t)P->g.W * P->bytes, P->g.H,
                          cudaMemcpyDeviceToHost, st), "result download");
     CK(cudaStreamSynchronize(st), "synchronize");
+    if (P->d_err) {
+      int flag = 0;
+      CK(cudaMemcpy(&flag, P->d_err, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
+      if (flag) return fail(FFT3D_E_CUDA, "neo_fft3d: tensor-core MMA completion wait timed out");
+    }
   }
   return FFT3D_OK;
 }
@@ -524,7 +539,7 @@ int fft3d_plane_create(const fft3d_params* p, const fft3d_plane_desc* d, int dev
   {
     const char* f = std::getenv("NEO_FFT3D_PATH");
     std::string v = f ? f : "unfused";
-    P->path = v == "fused" ? 2 : (v == "split" ? 0 : 1);
+    P->path = v == "fused" ? 2 : (v == "split" ? 0 : (v == "tc" ? 3 : 1));
   }
   fft3d_params& ep = P->ep;
   if (d->bits < 8 || (d->bits > 16 && d->bits != 32)) { delete P; return fail(FFT3D_E_PARAM, "neo_fft3d: unsupported bit depth"); }
@@ -672,6 +687,15 @@ int fft3d_plane_create(const fft3d_params* p, const fft3d_plane_desc* d, int dev
   for (auto& s : P->slots) {
     if (cudaMalloc(&s.spec, P->spec_elems() * sizeof(float2)) != cudaSuccess)
       return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (spectrum ring)"));
+  }
+  if (P->path == 3 && ep.bw == 32 && ep.bh == 32) {
+    std::vector<uint8_t> tc(fft3d::forward_tc_table_bytes());
+    fft3d::forward_tc_tables(wx.data(), wy.data(), tc.data());
+    if (cudaMalloc(&P->d_tc, tc.size()) != cudaSuccess || cudaMalloc(&P->d_err, sizeof(int)) != cudaSuccess)
+      return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (tensor-core tables)"));
+    if (cudaMemcpy(P->d_tc, tc.data(), tc.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(P->d_err, 0, sizeof(int)) != cudaSuccess)
+      return bail(fail(FFT3D_E_CUDA, "neo_fft3d: tensor-core table upload failed"));
   }
   if (P->path == 0 && cudaMalloc(&P->d_filt, P->spec_elems() * sizeof(float2)) != cudaSuccess)
     return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (filtered spectrum)"));

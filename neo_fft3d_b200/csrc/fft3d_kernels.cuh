@@ -119,6 +119,15 @@ cudaError_t launch_fused(const FusedArgs& a, int mode, int bytes_per_sample, cud
 bool block_size_supported(int bw, int bh);
 cudaError_t upload_twiddles();  // every registered size, on the current device
 
+// Tensor-core forward transform of 32x32 blocks (fft3d_tc.cu): DFT tables for
+// the plane's analysis windows (forward_tc_table_bytes() bytes, built on the
+// host, copied to the device once), and the launcher. `err` receives 1 when a
+// bounded wait on the MMA completion barrier times out.
+uint32_t forward_tc_table_bytes();
+uint32_t forward_tc_smem_bytes();
+void forward_tc_tables(const float* wx, const float* wy, uint8_t* out);
+cudaError_t launch_forward_tc(const ForwardArgs& a, const void* tables, int* err, int bytes_per_sample, cudaStream_t s);
+
 // Sets the message returned by fft3d_last_error() on this thread.
 void set_last_error(const std::string& msg);
 
