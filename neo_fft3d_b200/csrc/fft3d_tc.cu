@@ -42,6 +42,14 @@ constexpr uint32_t kTmemCols = 128;  // stage 1: 2 x 32 columns, stage 2: 64 col
 // 8 rows x 8 bf16, chunk k/8 stored as R rows of 16 bytes)
 __device__ __forceinline__ uint32_t kmaj(int r, int k, int R) { return (uint32_t)(((k >> 3) * R + r) * 16 + (k & 7) * 2); }
 
+// Stage-2 operand layout: K chunks of the same 8-row group 144 bytes apart
+// (LBO, one 16-byte pad per chunk) and 8-row groups 8 x 144 bytes apart (SBO),
+// so that the 32 lanes storing one row's 64 K values hit 32 different banks.
+constexpr int A2_LBO = 144, A2_SBO = 8 * 144;
+__device__ __forceinline__ uint32_t kmaj2(int r, int k) {
+  return (uint32_t)((k >> 3) * A2_LBO + (r >> 3) * A2_SBO + (r & 7) * 16 + (k & 7) * 2);
+}
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
@@ -125,13 +133,14 @@ __device__ __forceinline__ float ld_sample<uint16_t>(const uint16_t* p) { return
 constexpr uint32_t SZ_B1 = 32 * 32 * 2;     // G hi / lo: N=32 x K=32
 constexpr uint32_t SZ_B2 = 64 * 64 * 2;     // F hi / lo: N=64 x K=64
 constexpr uint32_t SZ_A1 = 128 * 32 * 2;    // one M=128 sub-tile of V (hi or lo)
-constexpr uint32_t SZ_A2 = 128 * 64 * 2;    // Z columns (hi or lo)
+constexpr uint32_t SZ_A2 = 16 * A2_SBO;     // Z columns (hi or lo): 16 groups of 8 rows
 constexpr uint32_t OFF_B1H = 0, OFF_B1L = OFF_B1H + SZ_B1, OFF_B2H = OFF_B1L + SZ_B1, OFF_B2L = OFF_B2H + SZ_B2;
-constexpr uint32_t OFF_A1H = OFF_B2L + SZ_B2;              // 2 sub-tiles
-constexpr uint32_t OFF_A1L = OFF_A1H + 2 * SZ_A1;          // 2 sub-tiles
-constexpr uint32_t OFF_A2H = OFF_A1L + 2 * SZ_A1, OFF_A2L = OFF_A2H + SZ_A2;
+constexpr uint32_t OFF_A2H = OFF_B2L + SZ_B2, OFF_A2L = OFF_A2H + SZ_A2;
 constexpr uint32_t OFF_BAR = OFF_A2L + SZ_A2;
-constexpr uint32_t SMEM_TC = OFF_BAR + 64;
+constexpr uint32_t OFF_A1H = OFF_BAR + 64;                 // 2 sub-tiles
+constexpr uint32_t OFF_A1L = OFF_A1H + 2 * SZ_A1;          // 2 sub-tiles, only when V is split
+constexpr uint32_t SMEM_TC = OFF_A1H + 2 * SZ_A1;          // V exact (8-bit samples)
+constexpr uint32_t SMEM_TC_SPLIT = OFF_A1L + 2 * SZ_A1;    // V split (9..16-bit, float)
 constexpr uint32_t TABLE_BYTES = 2 * SZ_B1 + 2 * SZ_B2;    // global image of B1h, B1l, B2h, B2l
 
 template <typename T, bool VSPLIT>
@@ -184,7 +193,25 @@ __global__ void __launch_bounds__(THREADS) k_forward_tc(ForwardArgs a, const uin
         const int x0 = bx * g.sx - g.sx;
         const float wy = 1.f;  // the y window is folded into stage 2
         (void)wy;
-        if (x0 >= 0 && x0 + TB <= g.W) {
+        const T* p = srow + x0;
+        if (x0 >= 0 && x0 + TB <= g.W && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+          // 16-byte loads of the row (the common interior case)
+          constexpr int PER = 16 / (int)sizeof(T);
+          const uint4* q = reinterpret_cast<const uint4*>(p);
+#pragma unroll
+          for (int c = 0; c < TB / PER; c++) {
+            const uint4 u = __ldg(q + c);
+            const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+            for (int j = 0; j < PER; j++) {
+              float f;
+              if constexpr (sizeof(T) == 1) f = (float)((w[j >> 2] >> (8 * (j & 3))) & 0xffu);
+              else if constexpr (sizeof(T) == 2) f = (float)((w[j >> 1] >> (16 * (j & 1))) & 0xffffu);
+              else f = __uint_as_float(w[j]);
+              v[c * PER + j] = f - a.base;
+            }
+          }
+        } else if (x0 >= 0 && x0 + TB <= g.W) {
 #pragma unroll
           for (int x = 0; x < TB; x++) v[x] = ld_sample<T>(srow + x0 + x) - a.base;
         } else {
@@ -247,8 +274,8 @@ __global__ void __launch_bounds__(THREADS) k_forward_tc(ForwardArgs a, const uin
         split_bf16(re, rh, rl);
         split_bf16(im, ih, il);
         const int m2 = b * 16 + c;
-        *reinterpret_cast<__nv_bfloat162*>(sm + OFF_A2H + kmaj(m2, 2 * y, 128)) = __halves2bfloat162(rh, ih);
-        *reinterpret_cast<__nv_bfloat162*>(sm + OFF_A2L + kmaj(m2, 2 * y, 128)) = __halves2bfloat162(rl, il);
+        *reinterpret_cast<__nv_bfloat162*>(sm + OFF_A2H + kmaj2(m2, 2 * y)) = __halves2bfloat162(rh, ih);
+        *reinterpret_cast<__nv_bfloat162*>(sm + OFF_A2L + kmaj2(m2, 2 * y)) = __halves2bfloat162(rl, il);
       }
     }
     fence_async_smem();
@@ -258,8 +285,8 @@ __global__ void __launch_bounds__(THREADS) k_forward_tc(ForwardArgs a, const uin
     if (tid == 0) {
       constexpr uint32_t id2 = idesc_bf16(128, 64);
       for (int ks = 0; ks < 4; ks++) {  // K = 64
-        const uint64_t dah = sdesc(sbase + OFF_A2H + ks * 2 * 128 * 16, 128 * 16, 128);
-        const uint64_t dal = sdesc(sbase + OFF_A2L + ks * 2 * 128 * 16, 128 * 16, 128);
+        const uint64_t dah = sdesc(sbase + OFF_A2H + ks * 2 * A2_LBO, A2_LBO, A2_SBO);
+        const uint64_t dal = sdesc(sbase + OFF_A2L + ks * 2 * A2_LBO, A2_LBO, A2_SBO);
         const uint64_t dbh = sdesc(sbase + OFF_B2H + ks * 2 * 64 * 16, 64 * 16, 128);
         const uint64_t dbl = sdesc(sbase + OFF_B2L + ks * 2 * 64 * 16, 64 * 16, 128);
         mma_bf16(d2, dah, dbh, id2, ks > 0 ? 1u : 0u);
@@ -275,29 +302,37 @@ __global__ void __launch_bounds__(THREADS) k_forward_tc(ForwardArgs a, const uin
     }
     phase ^= 1;
     tc_fence_after();
-    // ---- outputs: row m2 = (block, column) holds Y[h] (re, im) interleaved
+    // ---- outputs: row m2 = (block, column) holds Y[h] (re, im) interleaved;
+    // staged in shared memory (the stage-2 operands are free now) as the
+    // tile's contiguous spectra, then written with 16-byte stores
+    float2* stage = reinterpret_cast<float2*>(sm + OFF_A2H);
     {
       float y0[32], y1[32];
       tmem_ld32(d2 + ((uint32_t)(warp * 32) << 16), y0);       // h = 0..15
       tmem_ld32(d2 + ((uint32_t)(warp * 32) << 16) + 32, y1);  // h = 16..31
-      const int m2 = warp * 32 + lane, b = m2 >> 4, c = m2 & 15, blk = blk0 + b;
-      if (blk < g.nblocks) {
-        float2* out = a.spec + (size_t)blk * TB * NH;
-        auto Y = [&](int h) { return h < 16 ? make_float2(y0[2 * h], y0[2 * h + 1]) : make_float2(y1[2 * h - 32], y1[2 * h - 31]); };
-        if (c == 0) {
-          // unpack the DC (col 0) and Nyquist (col 16) transforms:
-          // A[h] = (Y[h] + conj Y[-h]) / 2, B[h] = (Y[h] - conj Y[-h]) / (2i)
+      const int m2 = warp * 32 + lane, b = m2 >> 4, c = m2 & 15;
+      float2* out = stage + b * TB * NH;
+      auto Y = [&](int h) { return h < 16 ? make_float2(y0[2 * h], y0[2 * h + 1]) : make_float2(y1[2 * h - 32], y1[2 * h - 31]); };
+      if (c == 0) {
+        // unpack the DC (col 0) and Nyquist (col 16) transforms:
+        // A[h] = (Y[h] + conj Y[-h]) / 2, B[h] = (Y[h] - conj Y[-h]) / (2i)
 #pragma unroll
-          for (int h = 0; h < TB; h++) {
-            const float2 yh = Y(h), ym = Y((TB - h) & (TB - 1));
-            out[h * NH] = make_float2(0.5f * (yh.x + ym.x), 0.5f * (yh.y - ym.y));
-            out[h * NH + 16] = make_float2(0.5f * (yh.y + ym.y), -0.5f * (yh.x - ym.x));
-          }
-        } else {
-#pragma unroll
-          for (int h = 0; h < TB; h++) out[h * NH + c] = Y(h);
+        for (int h = 0; h < TB; h++) {
+          const float2 yh = Y(h), ym = Y((TB - h) & (TB - 1));
+          out[h * NH] = make_float2(0.5f * (yh.x + ym.x), 0.5f * (yh.y - ym.y));
+          out[h * NH + 16] = make_float2(0.5f * (yh.y + ym.y), -0.5f * (yh.x - ym.x));
         }
+      } else {
+#pragma unroll
+        for (int h = 0; h < TB; h++) out[h * NH + c] = Y(h);
       }
+    }
+    __syncthreads();
+    {
+      const int nvalid = min(TILE, g.nblocks - blk0);
+      const uint4* src = reinterpret_cast<const uint4*>(stage);
+      uint4* dst = reinterpret_cast<uint4*>(a.spec + (size_t)blk0 * TB * NH);
+      for (int i = tid; i < nvalid * TB * NH / 2; i += THREADS) dst[i] = src[i];
     }
     tc_fence_before();
     __syncthreads();  // TMEM and smem operands are reused by the next tile
@@ -311,7 +346,7 @@ __global__ void __launch_bounds__(THREADS) k_forward_tc(ForwardArgs a, const uin
 }  // namespace
 
 uint32_t forward_tc_table_bytes() { return TABLE_BYTES; }
-uint32_t forward_tc_smem_bytes() { return SMEM_TC; }
+uint32_t forward_tc_smem_bytes() { return SMEM_TC_SPLIT; }
 
 // DFT tables of the tensor-core forward transform for a 32x32 block with
 // analysis windows wx, wy, in the global image layout the kernel copies to
@@ -356,18 +391,20 @@ cudaError_t launch_forward_tc(const ForwardArgs& a, const void* tables, int* err
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int ntiles = (a.g.nblocks + TILE - 1) / TILE;
-  const int grid = ntiles < sms * 3 ? ntiles : sms * 3;
+  const int per_sm = bytes == 1 ? 3 : 2;  // shared memory limits co-resident CTAs
+  const int grid = ntiles < sms * per_sm ? ntiles : sms * per_sm;
   const uint8_t* t = static_cast<const uint8_t*>(tables);
   cudaError_t e = cudaSuccess;
   if (bytes == 1) {
     e = cudaFuncSetAttribute(k_forward_tc<uint8_t, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_TC);
     if (e == cudaSuccess) k_forward_tc<uint8_t, false><<<grid, THREADS, SMEM_TC, s>>>(a, t, err);
   } else if (bytes == 2) {
-    e = cudaFuncSetAttribute(k_forward_tc<uint16_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_TC);
-    if (e == cudaSuccess) k_forward_tc<uint16_t, true><<<grid, THREADS, SMEM_TC, s>>>(a, t, err);
+    e = cudaFuncSetAttribute(k_forward_tc<uint16_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             SMEM_TC_SPLIT);
+    if (e == cudaSuccess) k_forward_tc<uint16_t, true><<<grid, THREADS, SMEM_TC_SPLIT, s>>>(a, t, err);
   } else {
-    e = cudaFuncSetAttribute(k_forward_tc<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_TC);
-    if (e == cudaSuccess) k_forward_tc<float, true><<<grid, THREADS, SMEM_TC, s>>>(a, t, err);
+    e = cudaFuncSetAttribute(k_forward_tc<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_TC_SPLIT);
+    if (e == cudaSuccess) k_forward_tc<float, true><<<grid, THREADS, SMEM_TC_SPLIT, s>>>(a, t, err);
   }
   return e != cudaSuccess ? e : cudaGetLastError();
 }
