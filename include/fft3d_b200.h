@@ -148,6 +148,93 @@ int fft3d_plane_timing(fft3d_plane* h, double out[15]);
 int fft3d_filter2d_static(const fft3d_params* p, const fft3d_plane_desc* d, const void* src, int src_stride,
                           void* dst, int dst_stride, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Learned noise PSD. No counterpart in the reference, whose per-frequency
+ * noise comes from sigma..sigma4 (src/helper.cpp:14-44) or from one measured
+ * block (src/helper.cpp:46-132) and enters the Wiener gain through the
+ * `pattern` slot (pattern2d, and pattern3d = bt x pattern2d,
+ * src/helper.cpp:171-178, src/fft3d_engine.h:625-630). This model predicts,
+ * for every 32x32 block, that slot's per-frequency noise power from the
+ * block's own log power spectrum: a 3-layer MLP (544 -> 512 -> 512 -> 544 bins,
+ * GELU, BF16 weights and activations, FP32 accumulation on the tensor cores,
+ * FP32 master weights, Adam), trained on the device from noisy/clean block
+ * pairs that the device generates (coloured Gaussian noise shaped by a random
+ * radially symmetric transfer function over seeded sinusoid-field frames).
+ * Units: |X|^2 of the plane's windowed, unnormalised block FFT.
+ * ------------------------------------------------------------------------ */
+typedef struct fft3d_psd fft3d_psd;
+
+#define FFT3D_PSD_BINS 544     /* 32 rows x 17 columns of a 32x32 block's half spectrum */
+#define FFT3D_PSD_FEATURES 576 /* model input width: BINS padded to a multiple of 64 */
+#define FFT3D_PSD_HIDDEN 512
+#define FFT3D_PSD_OUTPUTS 640  /* model output width: BINS padded to a multiple of 128 */
+#define FFT3D_PSD_INFO 12      /* floats of generator record per block, see fft3d_psd_generate */
+
+typedef struct fft3d_psd_train_cfg {
+  long long blocks;            /* training blocks generated on the device (default 2^21) */
+  int batch;                   /* rows per Adam step, a multiple of 128 (default 4096) */
+  int epochs;                  /* passes over the generated blocks (default 3) */
+  float lr, lr_final;          /* Adam step size, decayed linearly to lr_final */
+  unsigned long long seed;     /* data seed (weights are seeded at creation) */
+  int clean_frames;            /* clean frames generated at width x height (default 16) */
+  int width, height;           /* default 1920 x 1080 */
+  float sigma_min, sigma_max;  /* total noise sigma range in 8-bit codes (default 2, 10) */
+  float knot_min;              /* smallest transfer-function knot amplitude (default 0.1) */
+} fft3d_psd_train_cfg;
+
+void fft3d_psd_train_default(fft3d_psd_train_cfg* cfg);
+
+/* A model for 32x32 blocks with the analysis window of (ow, oh, wintype),
+ * weights initialised from `seed` (normal, std 1/sqrt(fan-in); zero biases). */
+int fft3d_psd_create(int device, unsigned long long seed, int ow, int oh, int wintype, fft3d_psd** out);
+void fft3d_psd_destroy(fft3d_psd* m);
+
+/* Parameters as FP32: W1 [512][576], b1 [512], W2 [512][512], b2 [512],
+ * W3 [640][512], b3 [640] (row = output unit), in that order. Input and output
+ * columns past 544 are padding (zero features; ignored outputs). */
+long long fft3d_psd_param_count(void);
+int fft3d_psd_get_params(fft3d_psd* m, float* host, long long n);
+int fft3d_psd_set_params(fft3d_psd* m, const float* host, long long n);
+
+/* Generate cfg->blocks training blocks on the device and train for
+ * cfg->epochs. loss_curve (may be NULL) receives the mean training loss of
+ * curve_len equal stretches of the run; val_loss (may be NULL) the loss on
+ * 32768 held-out blocks after training. */
+int fft3d_psd_train(fft3d_psd* m, const fft3d_psd_train_cfg* cfg, float* loss_curve, int curve_len, float* val_loss);
+
+/* The generator's blocks first .. first+count-1 of a training run with cfg,
+ * copied to HOST arrays (each may be NULL): features [count][576] (the BF16
+ * model input as float), target [count][544] (log noise power minus 7),
+ * info [count][12] (total sigma, knot amplitudes a0..a3 at radius 0, 1/3,
+ * 2/3, 1, direction (0 falling, 1 rising), noise gain s, clean frame, x0, y0,
+ * sum of FIR taps squared, 0), clean [count][1024] (unrounded clean pixels),
+ * noisy [count][1024] (8-bit noisy pixels). */
+int fft3d_psd_generate(fft3d_psd* m, const fft3d_psd_train_cfg* cfg, long long first, long long count,
+                       float* features, float* target, float* info, float* clean, unsigned char* noisy);
+
+/* One forward and backward pass on HOST rows (rows a multiple of 128):
+ * features [rows][576], target [rows][544]; writes the loss (mean squared
+ * error of the 544 outputs) and the gradients in the parameter layout. */
+int fft3d_psd_gradients(fft3d_psd* m, const float* features, const float* target, int rows, float* grads,
+                        float* loss);
+
+/* Model output for HOST feature rows: out [rows][544] (log noise power minus 7). */
+int fft3d_psd_forward(fft3d_psd* m, const float* features, int rows, float* out);
+
+/* Use the model's prediction in place of sigma for this plane: every output
+ * frame, the current frame's block spectra go through the model and the
+ * Wiener (or Kalman) noise power of block b, bin k becomes strength x its
+ * prediction (x bt for Wiener 3D, like pattern3d). The limited Wiener gain
+ * max(1 - noise/|F|^2, lowlimit) leaves part of every pure-noise bin when
+ * given the exact noise power; over-subtraction by strength ~3 maximises
+ * PSNR on the generator's noise (as the best scalar sigma does for white
+ * noise, whose sigma^2 / norm is ~3.4x the windowed noise power at bw = 32,
+ * ow = 16). pooled = 1 uses the mean log prediction of all blocks of the
+ * frame for every block. The plane must have bw = bh = 32 and the model's
+ * window; the model must outlive the plane's use of it. m = NULL returns to
+ * sigma. */
+int fft3d_plane_set_psd(fft3d_plane* h, fft3d_psd* m, int pooled, float strength);
+
 /* Message of the last failure on this thread ("" if none). */
 const char* fft3d_last_error(void);
 

@@ -17,6 +17,7 @@
 
 #include "fft3d_b200.h"
 #include "fft3d_kernels.cuh"
+#include "fft3d_psd.h"
 
 using fft3d::Geom;
 
@@ -100,6 +101,13 @@ struct fft3d_plane {
   uint8_t* d_tc = nullptr;  // tensor-core DFT tables (path 3)
   int* d_err = nullptr;     // device error flag of the tensor-core kernels
   float2* d_filt = nullptr;
+  // learned noise PSD (fft3d_plane_set_psd): model, per-block noise power, scratch
+  fft3d_psd* psd_model = nullptr;
+  int psd_pooled = 0;
+  float psd_pow = 1.f;
+  float psd_strength = 1.f;
+  float* d_psd = nullptr;
+  fft3d::psd::Work* psd_work = nullptr;
   bool timing = false;
   std::vector<Timed> pending;
   std::vector<cudaEvent_t> event_pool;
@@ -253,6 +261,8 @@ void free_plane(fft3d_plane* P) {
   cudaFree(P->d_last);
   cudaFree(P->d_cov);
   cudaFree(P->d_covp);
+  cudaFree(P->d_psd);
+  fft3d::psd::work_destroy(P->psd_work);
   cudaFree(P->d_in);
   cudaFree(P->d_out);
   if (P->stream) cudaStreamDestroy(P->stream);
@@ -363,12 +373,13 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
     P->pattern3d_init = true;
   }
   const int mode = bt > 0 ? btcur : bt;
+  const bool learned = P->psd_model && mode != fft3d::MODE_SHARPEN_ONLY;
   fft3d::InverseArgs ia{};
   // The steady state computes one new spectrum per output frame, the newest
   // of the window, in the fused kernel; older frames missing from the ring
   // (clip start, seeks) are transformed first by the forward kernel.
   const int newest = n + to;
-  const bool fused = P->path == 2 && P->bytes != 4 && !find_slot(P, newest);
+  const bool fused = P->path == 2 && P->bytes != 4 && !learned && !find_slot(P, newest);
   for (int d = from; d <= (fused ? to - 1 : to); d++) {
     Slot* s = nullptr;
     int rc = spectrum_slot(P, n + d, n + from, n + to, src ? src[2 + d] : nullptr, stride ? stride[2 + d] : 0, host,
@@ -411,8 +422,19 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
   c.pattern = P->pattern ? 1 : 0;
   c.use_sharpen = ep.sharpen != 0;
   c.use_dehalo = ep.dehalo != 0;
-  c.fuse_sharpen = (mode == 1 && !P->pattern) ? 1 : 0;
-  c.do_sharpen = ((ep.sharpen != 0 || ep.dehalo != 0) && (mode != 1 || P->pattern)) ? 1 : 0;
+  // a learned noise power takes the pattern's place, sharpen included (:620-621)
+  c.fuse_sharpen = (mode == 1 && !P->pattern && !learned) ? 1 : 0;
+  c.do_sharpen = ((ep.sharpen != 0 || ep.dehalo != 0) && (mode != 1 || P->pattern || learned)) ? 1 : 0;
+  if (learned) {
+    // the model reads the current frame's block spectra
+    CK(fft3d::psd::infer(P->psd_model, P->psd_work, ia.in[2], P->g.nblocks, P->psd_pooled != 0, P->psd_pow, P->d_psd,
+                         st),
+       "learned noise PSD");
+    g_launches += P->psd_pooled ? 10 : 8;  // features, 3 x (GEMM, bias/GELU), output
+    ia.psd = P->d_psd;
+    ia.psd_scale = P->psd_strength * (mode >= 2 ? (float)btcur : 1.f);
+    ia.psd_per_block = P->psd_pooled ? 0 : 1;
+  }
   ia.kal_last = P->d_last;
   ia.kal_covar = P->d_cov;
   ia.kal_covarp = P->d_covp;
@@ -494,9 +516,10 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
     CK(cudaMemcpy2DAsync(hdst, dst_stride, ddst, P->out_pitch, (size_t)P->g.W * P->bytes, P->g.H,
                          cudaMemcpyDeviceToHost, st), "result download");
     CK(cudaStreamSynchronize(st), "synchronize");
-    if (P->d_err) {
+    for (int* flagp : {P->d_err, learned ? fft3d::psd::err_flag(P->psd_model) : nullptr}) {
+      if (!flagp) continue;
       int flag = 0;
-      CK(cudaMemcpy(&flag, P->d_err, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
+      CK(cudaMemcpy(&flag, flagp, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
       if (flag) return fail(FFT3D_E_CUDA, "neo_fft3d: tensor-core MMA completion wait timed out");
     }
   }
@@ -797,6 +820,39 @@ int fft3d_plane_set_pattern_frame(fft3d_plane* P, const void* src, int stride) {
   CK(cudaStreamSynchronize(P->stream), "synchronize");
   P->pattern_set = true;
   P->pattern3d_init = false;
+  return FFT3D_OK;
+}
+
+int fft3d_plane_set_psd(fft3d_plane* P, fft3d_psd* m, int pooled, float strength) {
+  if (!P) return fail(FFT3D_E_PARAM, "neo_fft3d: null handle");
+  if (m && !(strength > 0.f)) return fail(FFT3D_E_PARAM, "neo_fft3d: the learned noise strength must be positive");
+  std::lock_guard<std::mutex> lk(P->mu);
+  cudaSetDevice(P->device);
+  CK(cudaStreamSynchronize(P->stream), "synchronize");
+  if (!m) {
+    P->psd_model = nullptr;
+    return FFT3D_OK;
+  }
+  const std::string why =
+      fft3d::psd::check_plane(m, P->device, P->g.bw, P->g.bh, P->g.ow, P->g.oh, P->ep.wintype);
+  if (!why.empty()) return fail(FFT3D_E_UNSUPPORTED, "neo_fft3d: " + why);
+  if (!P->d_psd) {
+    if (cudaMalloc(&P->d_psd, P->spec_elems() * sizeof(float)) != cudaSuccess) {
+      cudaGetLastError();
+      P->d_psd = nullptr;
+      return fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory for the learned noise power");
+    }
+  }
+  if (!P->psd_work) {
+    P->psd_work = fft3d::psd::work_create(m, P->g.nblocks);
+    if (!P->psd_work) return fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory for the learned noise PSD");
+  }
+  // sample scale relative to 8-bit codes: 2^(bits-8) for integer samples, 1/255 for float
+  const double scale = P->bytes == 4 ? 1.0 / 255.0 : std::ldexp(1.0, P->d.bits - 8);
+  P->psd_pow = (float)(scale * scale);
+  P->psd_model = m;
+  P->psd_pooled = pooled ? 1 : 0;
+  P->psd_strength = strength;
   return FFT3D_OK;
 }
 

@@ -83,6 +83,10 @@ struct InverseArgs {
   float* kal_covar;       // covariance (identical for re and im, src/code_impl/Kalman.cpp:41-64)
   float* kal_covarp;      // process covariance
   float* tdom;            // blocks x bh x bw time-domain output
+  const float* psd;       // learned noise power (null: sigma / pattern): per block
+                          // [blocks][bh*nh] when psd_per_block, else [bh*nh]
+  float psd_scale;        // btcur for Wiener 3D (pattern3d = bt x pattern2d), else 1
+  int psd_per_block;
   int reverse;            // walk the blocks from the end (alternated per frame so
                           // that the blocks read last stay in L2 for the next frame)
 };

@@ -253,6 +253,11 @@ __device__ __forceinline__ void wiener(float& re, float& im, float noise, float 
   im *= f;
 }
 
+// Learned noise power of bin `bin` of the block at spectrum offset `off`.
+__device__ __forceinline__ float learned_noise(const InverseArgs& a, size_t off, int bin) {
+  return a.psd_scale * __ldg(a.psd + (a.psd_per_block ? off : 0) + bin);
+}
+
 // Filtered value of one bin from its values w[0..4] in frames n-2..n+2 (only
 // the window's entries are read). MODE: 1 = Wiener 2D, 2..5 = Wiener 3D,
 // 0 = Kalman (updates the state when `commit`), -1 = sharpen only (identity).
@@ -267,7 +272,10 @@ __device__ __forceinline__ float2 filter_vals(const InverseArgs& a, const float2
     float2 last = a.kal_last[off + bin];
     float cv = a.kal_covar[off + bin], cp = a.kal_covarp[off + bin];
     float sigma = a.c.sigma2n_2d;
-    if (a.c.pattern) {
+    if (a.psd) {
+      sigma = learned_noise(a, off, bin);
+      if (sigma < 1e-15f) sigma = 1e-15f;
+    } else if (a.c.pattern) {
       sigma = __ldg(a.t.pattern2d + bin);
       if (sigma < 1e-15f) sigma = 1e-15f;
     }
@@ -299,7 +307,7 @@ __device__ __forceinline__ float2 filter_vals(const InverseArgs& a, const float2
     }
     const float cr = cur.x - gc.x, ci = cur.y - gc.y;
     const float psd = cr * cr + ci * ci + 1e-15f;
-    const float noise = a.c.pattern ? __ldg(a.t.pattern2d + bin) : a.c.sigma2n;
+    const float noise = a.psd ? learned_noise(a, off, bin) : a.c.pattern ? __ldg(a.t.pattern2d + bin) : a.c.sigma2n;
     const float q = __fdividef(psd - noise, psd);
     float f = q > a.c.lowlimit ? q : a.c.lowlimit;
     if (a.c.fuse_sharpen) {
@@ -317,7 +325,7 @@ __device__ __forceinline__ float2 filter_vals(const InverseArgs& a, const float2
       g0 = gf * gs.x * kb;
       g1 = gf * gs.y * kb;
     }
-    const float noise = a.c.pattern ? __ldg(a.t.pattern3d + bin) : a.c.sigma2n;
+    const float noise = a.psd ? learned_noise(a, off, bin) : a.c.pattern ? __ldg(a.t.pattern3d + bin) : a.c.sigma2n;
     const float ll = a.c.lowlimit;
     const float cr = cur.x, ci = cur.y;
     if constexpr (MODE == 2) {

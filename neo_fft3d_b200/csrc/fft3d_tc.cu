@@ -252,9 +252,9 @@ __global__ void __launch_bounds__(THREADS) k_forward_tc(ForwardArgs a, const uin
       }
       mma_commit(bar);
     }
-    if (!mbar_wait(bar, phase)) {
+    if (__syncthreads_or(mbar_wait(bar, phase) ? 0 : 1)) {  // uniform verdict: no thread left at a barrier
       ok = false;
-      atomicOr(err, 1);
+      if (tid == 0) atomicOr(err, 1);
       break;
     }
     phase ^= 1;
@@ -295,9 +295,9 @@ __global__ void __launch_bounds__(THREADS) k_forward_tc(ForwardArgs a, const uin
       }
       mma_commit(bar);
     }
-    if (!mbar_wait(bar, phase)) {
+    if (__syncthreads_or(mbar_wait(bar, phase) ? 0 : 1)) {  // uniform verdict: no thread left at a barrier
       ok = false;
-      atomicOr(err, 1);
+      if (tid == 0) atomicOr(err, 1);
       break;
     }
     phase ^= 1;

@@ -51,6 +51,7 @@ def lib():
         L.fft3d_kernel_launches.restype = ctypes.c_uint64
         L.fft3d_plane_set_timing.argtypes = [vp, ci]
         L.fft3d_plane_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+        L.fft3d_plane_set_psd.argtypes = [vp, vp, ci, ctypes.c_float]
         _lib = L
     return _lib
 
@@ -110,6 +111,14 @@ class PlaneEngine:
         frame = np.ascontiguousarray(frame)
         _check(lib().fft3d_plane_set_pattern_frame(self.h, frame.ctypes.data, frame.strides[0]))
 
+    def set_psd(self, model, pooled: bool = False, strength: float = 3.0):
+        """Take the Wiener/Kalman noise power from a learned PSD model
+        (neo_fft3d_b200.psd.PsdModel), times `strength`, instead of sigma;
+        None returns to sigma."""
+        _check(lib().fft3d_plane_set_psd(self.h, model.h if model is not None else None, 1 if pooled else 0,
+                                         strength))
+        self._psd_model = model  # the model must outlive its use by this plane
+
     def set_timing(self, enable: bool):
         _check(lib().fft3d_plane_set_timing(self.h, 1 if enable else 0))
 
@@ -134,10 +143,12 @@ class PlaneEngine:
             pass
 
 
-def filter_clip(planes, frames=None, bits=None, device: int = 0, **kw):
+def filter_clip(planes, frames=None, bits=None, device: int = 0, psd=None, psd_pooled=False, psd_strength=3.0, **kw):
     """FFT3D(clip, **kw) on the GPU for a clip given as a list of [F,H,W] host
     planes, the way the plugin drives its engines: one engine per processed
-    plane, frames in order, unprocessed planes copied. Returns output planes."""
+    plane, frames in order, unprocessed planes copied. Returns output planes.
+    psd: a learned noise-PSD model used in place of sigma (PlaneEngine.set_psd),
+    with psd_pooled / psd_strength as there."""
     F = planes[0].shape[0]
     if bits is None:
         bits = 8 if planes[0].dtype == np.uint8 else (32 if planes[0].dtype == np.float32 else 16)
@@ -153,6 +164,8 @@ def filter_clip(planes, frames=None, bits=None, device: int = 0, **kw):
             outs.append(o)
             continue
         eng = PlaneEngine(p, descs[i], device)
+        if psd is not None:
+            eng.set_psd(psd, psd_pooled, psd_strength)
         if p.pfactor != 0:
             eng.set_pattern_frame(a[min(max(p.pframe, 0), F - 1)])
         for j, n in enumerate(frames):

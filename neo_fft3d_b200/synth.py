@@ -121,3 +121,86 @@ WORKLOADS = {
                                        scene_cut=30),
                              filt=dict(sigma=3.0, bt=0, kratio=2.0, bw=48, bh=48, ow=16, oh=16)),
 }
+
+
+# ---------------------------------------------------------------- coloured noise
+# Noise of the learned-PSD workload: white Gaussian noise shaped by a 16x16 FIR
+# whose frequency response samples a radially symmetric transfer function, a
+# monotone cubic (Fritsch-Carlson) spline through 4 knot amplitudes at
+# normalised radius 0, 1/3, 2/3, 1 (radius 1 = 0.5 cycles per pixel), scaled
+# to a total standard deviation sigma. The same process family trains the
+# model (on the GPU, per block) and makes the evaluation clips (here, per frame).
+
+FIR_TAPS = 16
+
+
+def _spline(v, r):
+    v = np.asarray(v, np.float64)
+    dl = (v[1:] - v[:-1]) * 3.0
+    m = np.array([dl[0], 0.0, 0.0, dl[2]])
+    for k in (1, 2):
+        m[k] = 0.0 if dl[k - 1] * dl[k] <= 0 else 0.5 * (dl[k - 1] + dl[k])
+    for k in range(3):
+        if dl[k] == 0:
+            m[k] = m[k + 1] = 0.0
+        else:
+            a, b = m[k] / dl[k], m[k + 1] / dl[k]
+            if a * a + b * b > 9.0:
+                tau = 3.0 / np.sqrt(a * a + b * b)
+                m[k], m[k + 1] = tau * a * dl[k], tau * b * dl[k]
+    i = np.minimum(2, (r * 3.0).astype(int))
+    t = (r - i / 3.0) * 3.0
+    return ((2 * t ** 3 - 3 * t ** 2 + 1) * v[i] + (t ** 3 - 2 * t ** 2 + t) / 3.0 * m[i]
+            + (-2 * t ** 3 + 3 * t ** 2) * v[i + 1] + (t ** 3 - t ** 2) / 3.0 * m[i + 1])
+
+
+def noise_fir(knots) -> np.ndarray:
+    """Centred 16x16 FIR (tap [a][b] at lag (a-8, b-8)) of the transfer
+    function with the given 4 monotone knot amplitudes."""
+    n = FIR_TAPS
+    f = np.array([(i if i <= n // 2 else i - n) / n for i in range(n)])
+    r = np.minimum(1.0, 2.0 * np.sqrt(f[:, None] ** 2 + f[None, :] ** 2))
+    h = np.real(np.fft.ifft2(_spline(knots, r)))
+    return np.roll(h, (n // 2, n // 2), axis=(0, 1))
+
+
+def coloured_noise(frames: int, height: int, width: int, knots, sigma: float, seed: int = 0) -> np.ndarray:
+    """[frames, height, width] float64 coloured noise of total std sigma."""
+    from scipy.signal import correlate
+    h = noise_fir(knots)
+    gain = sigma / np.sqrt(np.sum(h * h))
+    rng = np.random.default_rng([seed, 300])
+    out = np.empty((frames, height, width))
+    for t in range(frames):
+        w = rng.standard_normal((height + FIR_TAPS - 1, width + FIR_TAPS - 1))
+        out[t] = gain * correlate(w, h, mode="valid", method="fft")
+    return out
+
+
+def make_coloured_clip(width: int, height: int, frames: int, knots, sigma: float, seed: int = 0):
+    """Luma-only 8-bit clip of the sinusoid field (as make_clip) plus coloured
+    noise; returns (noisy, clean) uint8 arrays [frames, height, width]."""
+    v = _field_values(width, height, frames, seed)
+    noisy = np.clip(np.rint(v + coloured_noise(frames, height, width, knots, sigma, seed)), 0, 255).astype(np.uint8)
+    return noisy, np.clip(np.rint(v), 0, 255).astype(np.uint8)
+
+
+def _field_values(width: int, height: int, frames: int, seed: int) -> np.ndarray:
+    """Unrounded luma values of make_clip's field (no noise)."""
+    rng_motion = np.random.default_rng([seed, 1])
+    steps = rng_motion.uniform(-2.0, 2.0, size=(frames, 2))
+    steps[0] = 0.0
+    path = np.cumsum(steps, axis=0)
+    params = _field_params(np.random.default_rng([seed, 10]))
+    f0 = _eval_field(params, width, height, 0.0, 0.0, 1.0)
+    fmin, fmax = f0.min(), f0.max()
+    out = np.empty((frames, height, width))
+    for t in range(frames):
+        f = _eval_field(params, width, height, path[t][0], path[t][1], 1.0)
+        out[t] = 16 + (f - fmin) * ((235 - 16) / (fmax - fmin))
+    return out
+
+
+def psnr(a: np.ndarray, b: np.ndarray, peak: float = 255.0) -> float:
+    d = a.astype(np.float64) - b.astype(np.float64)
+    return float(10 * np.log10(peak * peak / np.mean(d * d)))
