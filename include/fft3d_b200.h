@@ -202,6 +202,11 @@ int fft3d_psd_set_params(fft3d_psd* m, const float* host, long long n);
  * 32768 held-out blocks after training. */
 int fft3d_psd_train(fft3d_psd* m, const fft3d_psd_train_cfg* cfg, float* loss_curve, int curve_len, float* val_loss);
 
+/* Device timing of the last fft3d_psd_train: out[0] ms generating the blocks,
+ * out[1] ms of the training steps, out[2] steps, out[3] GEMM flops per step
+ * (forward + backward). */
+int fft3d_psd_train_stats(fft3d_psd* m, double out[4]);
+
 /* The generator's blocks first .. first+count-1 of a training run with cfg,
  * copied to HOST arrays (each may be NULL): features [count][576] (the BF16
  * model input as float), target [count][544] (log noise power minus 7),

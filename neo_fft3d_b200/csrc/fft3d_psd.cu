@@ -485,6 +485,7 @@ struct fft3d_psd {
   int* err = nullptr;
   float* loss = nullptr;  // device scalar
   int step = 0;           // Adam steps taken
+  double stats[4] = {};   // last training run: generation ms, training ms, steps, GEMM flops per step
 };
 
 namespace {
@@ -930,7 +931,10 @@ int fft3d_psd_train(fft3d_psd* m, const fft3d_psd_train_cfg* c, float* loss_curv
     cudaFree(minmax);
     return fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory for the training blocks");
   }
+  cudaEvent_t ev[3] = {};
+  for (auto& x : ev) cudaEventCreate(&x);
   cudaError_t e = cudaMemsetAsync(losses, 0, (steps + 1) * 4, m->stream);
+  cudaEventRecord(ev[0], m->stream);
   // the training blocks, then the held-out blocks (indices after them)
   for (long long s0 = 0; s0 < total && e == cudaSuccess; s0 += 1 << 20) {
     GenArgs g = gen_args(m, c, field, minmax, s0, std::min<long long>(1 << 20, total - s0));
@@ -938,6 +942,7 @@ int fft3d_psd_train(fft3d_psd* m, const fft3d_psd_train_cfg* c, float* loss_curv
     g.T = T + s0 * BINS;
     e = launch_gen(g, m->stream);
   }
+  cudaEventRecord(ev[1], m->stream);
   for (long long s = 0; s < steps && e == cudaSuccess; s++) {
     const long long b = s % nb;
     const __nv_bfloat16* xb = X + b * c->batch * IN;
@@ -949,6 +954,7 @@ int fft3d_psd_train(fft3d_psd* m, const fft3d_psd_train_cfg* c, float* loss_curv
     if (e == cudaSuccess)
       e = fft3d::mlp::adam(m->w, m->g, m->m1, m->m2, m->wb, NPARAM, lr, 0.9f, 0.999f, 1e-8f, ++m->step, m->stream);
   }
+  cudaEventRecord(ev[2], m->stream);
   // held-out loss
   const long long vchunks = kValBlocks / c->batch;
   for (long long k = 0; k < vchunks && e == cudaSuccess; k++) {
@@ -961,6 +967,18 @@ int fft3d_psd_train(fft3d_psd* m, const fft3d_psd_train_cfg* c, float* loss_curv
   if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
   std::vector<float> hl(steps + 1, 0.f);
   if (e == cudaSuccess) e = cudaMemcpy(hl.data(), losses, (steps + 1) * 4, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) {
+    float g_ms = 0.f, t_ms = 0.f;
+    cudaEventElapsedTime(&g_ms, ev[0], ev[1]);
+    cudaEventElapsedTime(&t_ms, ev[1], ev[2]);
+    // forward 1x, backward 2x the forward's GEMM flops
+    const double fwd = 2.0 * c->batch * ((double)IN * HID + (double)HID * HID + (double)HID * OUT);
+    m->stats[0] = g_ms;
+    m->stats[1] = t_ms;
+    m->stats[2] = (double)steps;
+    m->stats[3] = 3.0 * fwd;
+  }
+  for (auto& x : ev) cudaEventDestroy(x);
   work_free(w);
   cudaFree(X);
   cudaFree(T);
@@ -979,6 +997,13 @@ int fft3d_psd_train(fft3d_psd* m, const fft3d_psd_train_cfg* c, float* loss_curv
     }
   }
   if (val_loss) *val_loss = vchunks > 0 ? hl[steps] / (float)vchunks : 0.f;
+  return FFT3D_OK;
+}
+
+int fft3d_psd_train_stats(fft3d_psd* m, double out[4]) {
+  if (!m || !out) return fail(FFT3D_E_PARAM, "neo_fft3d: null argument");
+  std::lock_guard<std::mutex> lk(m->mu);
+  std::copy(m->stats, m->stats + 4, out);
   return FFT3D_OK;
 }
 

@@ -42,6 +42,7 @@ def _bind():
         L.fft3d_psd_generate.argtypes = [vp, cfgp, ll, ll, vp, vp, vp, vp, vp]
         L.fft3d_psd_gradients.argtypes = [vp, vp, vp, ci, vp, fp]
         L.fft3d_psd_forward.argtypes = [vp, vp, ci, vp]
+        L.fft3d_psd_train_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         _bound = True
     return L
 
@@ -93,6 +94,13 @@ class PsdModel:
         val = ctypes.c_float()
         _check(_bind().fft3d_psd_train(self.h, ctypes.byref(cfg), curve.ctypes.data, curve_len, ctypes.byref(val)))
         return curve, float(val.value)
+
+    def train_stats(self) -> dict:
+        """Device timing of the last train(): generation and training ms,
+        steps, GEMM flops per step."""
+        out = (ctypes.c_double * 4)()
+        _check(_bind().fft3d_psd_train_stats(self.h, out))
+        return dict(generate_ms=out[0], train_ms=out[1], steps=int(out[2]), gemm_flops_per_step=out[3])
 
     def generate(self, first: int, count: int, cfg: TrainCfg | None = None, **kw) -> dict:
         """The generator's blocks first .. first+count-1 (host copies)."""
