@@ -149,6 +149,41 @@ int fft3d_filter2d_static(const fft3d_params* p, const fft3d_plane_desc* d, cons
                           void* dst, int dst_stride, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Batched multi-plane scheduler. No counterpart in the reference, which runs
+ * one FFT3DEngine per plane per clip (src/fft3d.hpp:186-198, 241). One step
+ * filters one output frame of each of `count` planes -- luma and chroma of
+ * many clips, of mixed sizes, block sizes, bt and sample types -- with one
+ * batched persistent launch per kernel variant and phase (forward,
+ * filter/inverse, overlap-add) instead of three launches per plane. The
+ * first steps of a new step shape are timed under candidate schedules
+ * (persistent grid size, work-item order) and the fastest is kept per
+ * launch (autotuner); the tuned step is captured into a CUDA graph and
+ * replayed on later steps of that shape.
+ * ------------------------------------------------------------------------ */
+typedef struct fft3d_batch fft3d_batch;
+
+int fft3d_batch_create(int device, fft3d_batch** out);
+void fft3d_batch_destroy(fft3d_batch* b);
+
+/* 1 (default): tune new step shapes; 0: use the default schedule (all
+ * resident CTAs per SM, plane-major work items). */
+int fft3d_batch_set_tuning(fft3d_batch* b, int enable);
+
+/* One step: plane i filters its output frame n[i] from DEVICE frames
+ * src[5*i + k] (frame n[i] + k - 2, strides src_stride[5*i + k] in bytes, as
+ * in fft3d_plane_filter_device) into dst[i] (stride dst_stride[i]); all work
+ * is queued on `stream` (a cudaStream_t) without a host synchronisation
+ * (except while a new step shape is tuned). Successive steps of one batch
+ * must use one stream. Planes must be on the batch's device, on the default
+ * (unfused) path, without a learned PSD; each plane at most once per step. */
+int fft3d_batch_step(fft3d_batch* b, int count, fft3d_plane* const* planes, const int* n, const void* const* src,
+                     const int* src_stride, void* const* dst, const int* dst_stride, void* stream);
+
+/* out[0] steps, [1] graph launches, [2] tuning steps, [3] 0, [4] kernels
+ * of the last step, [5] step shapes seen, [6..7] 0. */
+int fft3d_batch_stats(fft3d_batch* b, double out[8]);
+
+/* ------------------------------------------------------------------------
  * Learned noise PSD. No counterpart in the reference, whose per-frequency
  * noise comes from sigma..sigma4 (src/helper.cpp:14-44) or from one measured
  * block (src/helper.cpp:46-132) and enters the Wiener gain through the

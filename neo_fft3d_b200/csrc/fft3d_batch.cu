@@ -1,0 +1,469 @@
+// Batched multi-plane scheduler: one time step of many planes (luma and
+// chroma of many clips, mixed sizes, block sizes and bt) as one batched
+// persistent launch per kernel variant and phase, captured into a CUDA graph.
+//
+// A step plans every plane with the engine's own per-frame control (spectrum
+// ring, btcur edges, Kalman passthrough, crop) while the launches are
+// recorded instead of issued (fft3d::plane_plan). The records are grouped by
+// kernel variant -- forward by (bw, bh, sample type), filter/inverse by
+// (bw, bh, mode), plane copies, overlap-add by sample type -- and each group becomes ONE
+// launch whose CTAs walk a list of (plane, CTA-of-that-plane) work items, so
+// a step of 48 clips x 3 planes is ~3-12 launches instead of ~430.
+//
+// Autotuner. The step's shape (groups and their per-plane work items) is
+// its signature. The first steps of a new signature try each candidate
+// schedule -- persistent grid of 1, 2, 4 or all resident CTAs per SM, or one
+// CTA per work item; work items plane-major or interleaved across planes --
+// timing every group's launch with CUDA events, and keep the fastest
+// schedule per group. The tuned step is then captured once into a CUDA graph
+// (argument upload from pinned staging + the launches); later steps of that
+// signature only rewrite the pinned arguments and launch the graph. Two
+// graph instances alternate over two staging buffers so that the host can
+// prepare a step while the previous one runs.
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "fft3d_b200.h"
+#include "fft3d_batch.h"
+#include "fft3d_kernels.cuh"
+
+namespace {
+
+using fft3d::Deferred;
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fft3d::engine_fail(FFT3D_E_CUDA,
+                            std::string("neo_fft3d: CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+#define CK(call, what)                                 \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// candidate schedules: resident CTAs per SM of the persistent grid (0 = one
+// CTA per work item) x work-item order
+struct Sched {
+  int per_sm;
+  int interleave;
+};
+const Sched kCandidates[] = {{0, 0}, {1, 0}, {2, 0}, {4, 0}, {64, 0}, {0, 1}, {1, 1}, {2, 1}, {4, 1}, {64, 1}};
+constexpr int kNumCand = sizeof(kCandidates) / sizeof(kCandidates[0]);
+
+// phases in launch order; plane copies (crop borders, Kalman frame 0) go
+// before the overlap-add, which writes the interior over them
+enum Phase { PH_FWD = 0, PH_INV = 1, PH_COPY = 2, PH_OLA = 3 };
+
+struct Group {
+  int phase, bw, bh, var;   // var: bytes per sample (forward, overlap-add) or filter mode
+  std::vector<int> recs;    // indices into the Deferred vector of the phase
+  std::vector<int> per;     // work items per record
+  int nitems = 0;
+  int occupancy = 1;        // resident CTAs per SM
+  size_t args_off = 0, items_off = 0, arg_size = 0;
+  Sched sched{64, 0};
+  int grid = 1;
+};
+
+struct Plan {
+  std::vector<Group> groups;
+  std::string sig;
+  size_t args_bytes = 0, items_bytes = 0;
+};
+
+struct Tune {
+  int next = 0;                             // next candidate to try
+  std::vector<std::vector<float>> ms;      // [group][candidate]
+  bool done = false;
+  std::vector<Sched> best;
+};
+
+struct Captured {
+  void* d_buf = nullptr;      // device: args then items
+  void* h_stage[2] = {};      // pinned: args of a step
+  cudaGraphExec_t exec[2] = {};
+  cudaEvent_t done[2] = {};
+  bool used[2] = {};
+  int parity = 0;
+  ~Captured() {
+    for (int p = 0; p < 2; p++) {
+      if (exec[p]) cudaGraphExecDestroy(exec[p]);
+      if (done[p]) cudaEventDestroy(done[p]);
+      if (h_stage[p]) cudaFreeHost(h_stage[p]);
+    }
+    if (d_buf) cudaFree(d_buf);
+  }
+};
+
+size_t arg_size(int phase) {
+  switch (phase) {
+    case PH_FWD: return sizeof(fft3d::ForwardArgs);
+    case PH_INV: return sizeof(fft3d::InverseArgs);
+    case PH_COPY: return sizeof(fft3d::CopyArgs);
+    default: return sizeof(fft3d::OlaArgs);
+  }
+}
+
+const fft3d::Geom& rec_geom(const Deferred& d, int phase, int r) {
+  return phase == PH_FWD ? d.fwd[r].a.g : (phase == PH_INV ? d.inv[r].a.g : d.ola[r].a.g);
+}
+
+fft3d::CopyArgs copy_args(const Deferred::Copy& c) {
+  fft3d::CopyArgs a;
+  a.dst = c.dst;
+  a.dpitch = (long long)c.dpitch;
+  a.src = c.src;
+  a.spitch = (long long)c.spitch;
+  a.width = (long long)c.width;
+  a.height = (int)c.height;
+  return a;
+}
+
+}  // namespace
+
+struct fft3d_batch {
+  std::mutex mu;
+  int device = 0;
+  int sms = 148;
+  int tuning = 1;
+  cudaStream_t cap = nullptr;  // capture stream
+  std::map<std::string, Tune> tunes;
+  std::map<std::string, std::unique_ptr<Captured>> graphs;
+  void* d_direct = nullptr;
+  size_t d_direct_cap = 0;
+  void* h_direct = nullptr;
+  size_t h_direct_cap = 0;
+  cudaEvent_t direct_done = nullptr;
+  double stats[8] = {};  // steps, graph launches, tuning steps, -, kernels of the last step, step shapes
+};
+
+namespace {
+
+void build_groups(const Deferred& d, Plan& plan) {
+  std::map<std::tuple<int, int, int, int>, int> index;
+  auto add = [&](int phase, int r, int bw, int bh, int var) {
+    auto key = std::make_tuple(phase, bw, bh, var);
+    auto it = index.find(key);
+    int gi;
+    if (it == index.end()) {
+      gi = (int)plan.groups.size();
+      index[key] = gi;
+      Group g;
+      g.phase = phase;
+      g.bw = bw;
+      g.bh = bh;
+      g.var = var;
+      plan.groups.push_back(g);
+    } else {
+      gi = it->second;
+    }
+    Group& g = plan.groups[gi];
+    int items;
+    if (phase == PH_COPY) items = (int)d.copies[r].height;
+    else if (phase == PH_OLA) items = fft3d::batch_items_overlap_add(rec_geom(d, phase, r));
+    else items = fft3d::batch_items_forward(rec_geom(d, phase, r));
+    g.recs.push_back(r);
+    g.per.push_back(items);
+    g.nitems += items;
+  };
+  for (int r = 0; r < (int)d.fwd.size(); r++) add(PH_FWD, r, d.fwd[r].a.g.bw, d.fwd[r].a.g.bh, d.fwd[r].bytes);
+  for (int r = 0; r < (int)d.inv.size(); r++) add(PH_INV, r, d.inv[r].a.g.bw, d.inv[r].a.g.bh, d.inv[r].mode);
+  for (int r = 0; r < (int)d.copies.size(); r++) add(PH_COPY, r, 0, 0, 0);
+  for (int r = 0; r < (int)d.ola.size(); r++) add(PH_OLA, r, 0, 0, d.ola[r].bytes);
+  // phases in order; within a phase the larger groups first
+  std::stable_sort(plan.groups.begin(), plan.groups.end(), [](const Group& a, const Group& b) {
+    return a.phase != b.phase ? a.phase < b.phase : a.nitems > b.nitems;
+  });
+  std::string sig;
+  size_t off = 0;
+  for (auto& g : plan.groups) {
+    g.arg_size = arg_size(g.phase);
+    g.args_off = off;
+    off = align_up(off + g.arg_size * g.recs.size(), 256);
+    sig += std::to_string(g.phase) + "/" + std::to_string(g.bw) + "x" + std::to_string(g.bh) + "/" +
+           std::to_string(g.var) + ":";
+    for (int n : g.per) sig += std::to_string(n) + ",";
+    sig += ";";
+  }
+  plan.args_bytes = off;
+  for (auto& g : plan.groups) {
+    g.items_off = off;
+    off = align_up(off + sizeof(int2) * g.nitems, 256);
+  }
+  plan.items_bytes = off - plan.args_bytes;
+  plan.sig = sig;
+}
+
+void write_args(const Deferred& d, const Plan& plan, char* base) {
+  for (const auto& g : plan.groups) {
+    char* p = base + g.args_off;
+    for (size_t i = 0; i < g.recs.size(); i++) {
+      const int r = g.recs[i];
+      if (g.phase == PH_COPY) {
+        const fft3d::CopyArgs c = copy_args(d.copies[r]);
+        std::memcpy(p + i * g.arg_size, &c, g.arg_size);
+        continue;
+      }
+      const void* src = g.phase == PH_FWD ? (const void*)&d.fwd[r].a
+                                          : (g.phase == PH_INV ? (const void*)&d.inv[r].a : (const void*)&d.ola[r].a);
+      std::memcpy(p + i * g.arg_size, src, g.arg_size);
+    }
+  }
+}
+
+void write_items(const Plan& plan, char* base) {  // base: start of the items area
+  for (const auto& g : plan.groups) {
+    int2* it = reinterpret_cast<int2*>(base + (g.items_off - plan.args_bytes));
+    int k = 0;
+    if (!g.sched.interleave) {
+      for (size_t i = 0; i < g.recs.size(); i++)
+        for (int c = 0; c < g.per[i]; c++) it[k++] = make_int2((int)i, c);
+    } else {
+      const int most = *std::max_element(g.per.begin(), g.per.end());
+      for (int c = 0; c < most; c++)
+        for (size_t i = 0; i < g.recs.size(); i++)
+          if (c < g.per[i]) it[k++] = make_int2((int)i, c);
+    }
+  }
+}
+
+void set_grids(fft3d_batch* b, Plan& plan) {
+  for (auto& g : plan.groups) {
+    const int which = g.phase;
+    g.occupancy = fft3d::batch_occupancy(g.bw, g.bh, which, g.var);
+    const int per_sm = g.sched.per_sm == 0 ? 0 : std::min(g.sched.per_sm, g.occupancy);
+    g.grid = per_sm == 0 ? g.nitems : std::max(1, std::min(g.nitems, per_sm * b->sms));
+  }
+}
+
+cudaError_t launch_group(const Group& g, const char* d_base, cudaStream_t s) {
+  fft3d::BatchLaunch l;
+  l.args = d_base + g.args_off;
+  l.items = reinterpret_cast<const int2*>(d_base + g.items_off);
+  l.nitems = g.nitems;
+  l.grid = g.grid;
+  if (g.phase == PH_FWD) return fft3d::launch_forward_batch(g.bw, g.bh, l, g.var, s);
+  if (g.phase == PH_INV) return fft3d::launch_filter_inverse_batch(g.bw, g.bh, l, g.var, s);
+  if (g.phase == PH_COPY) return fft3d::launch_copy_batch(l, s);
+  return fft3d::launch_overlap_add_batch(l, g.var, s);
+}
+
+cudaError_t run_groups(const Plan& plan, const char* d_base, cudaStream_t s, std::vector<cudaEvent_t>* ev) {
+  for (size_t i = 0; i < plan.groups.size(); i++) {
+    if (ev) cudaEventRecord((*ev)[2 * i], s);
+    cudaError_t e = launch_group(plan.groups[i], d_base, s);
+    if (e != cudaSuccess) return e;
+    if (ev) cudaEventRecord((*ev)[2 * i + 1], s);
+  }
+  return cudaSuccess;
+}
+
+// A step without a graph: arguments and items through pinned staging.
+int run_direct(fft3d_batch* b, Plan& plan, const Deferred& d, cudaStream_t s, std::vector<cudaEvent_t>* ev) {
+  const size_t total = plan.args_bytes + plan.items_bytes;
+  if (b->direct_done) CK(cudaEventSynchronize(b->direct_done), "batch staging");
+  if (total > b->h_direct_cap) {
+    if (b->h_direct) cudaFreeHost(b->h_direct);
+    b->h_direct = nullptr;
+    CK(cudaMallocHost(&b->h_direct, total), "batch staging");
+    b->h_direct_cap = total;
+  }
+  if (total > b->d_direct_cap) {
+    if (b->d_direct) {
+      cudaStreamSynchronize(s);
+      cudaFree(b->d_direct);
+    }
+    b->d_direct = nullptr;
+    CK(cudaMalloc(&b->d_direct, total), "batch arguments");
+    b->d_direct_cap = total;
+  }
+  char* h = static_cast<char*>(b->h_direct);
+  write_args(d, plan, h);
+  write_items(plan, h + plan.args_bytes);
+  CK(cudaMemcpyAsync(b->d_direct, h, total, cudaMemcpyHostToDevice, s), "batch arguments");
+  CK(run_groups(plan, static_cast<const char*>(b->d_direct), s, ev), "batched launch");
+  if (!b->direct_done) CK(cudaEventCreateWithFlags(&b->direct_done, cudaEventDisableTiming), "batch event");
+  CK(cudaEventRecord(b->direct_done, s), "batch event");
+  return FFT3D_OK;
+}
+
+int capture(fft3d_batch* b, Plan& plan, Captured* c) {
+  const size_t total = plan.args_bytes + plan.items_bytes;
+  CK(cudaMalloc(&c->d_buf, total), "batch graph buffers");
+  std::vector<char> items(plan.items_bytes);
+  write_items(plan, items.data());
+  CK(cudaMemcpy(static_cast<char*>(c->d_buf) + plan.args_bytes, items.data(), plan.items_bytes,
+                cudaMemcpyHostToDevice),
+     "batch graph items");
+  for (int p = 0; p < 2; p++) {
+    CK(cudaMallocHost(&c->h_stage[p], plan.args_bytes), "batch graph staging");
+    CK(cudaEventCreateWithFlags(&c->done[p], cudaEventDisableTiming), "batch graph event");
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal), "batch graph capture");
+    cudaError_t e = cudaMemcpyAsync(c->d_buf, c->h_stage[p], plan.args_bytes, cudaMemcpyHostToDevice, b->cap);
+    if (e == cudaSuccess) e = run_groups(plan, static_cast<const char*>(c->d_buf), b->cap, nullptr);
+    cudaError_t e2 = cudaStreamEndCapture(b->cap, &graph);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      return cuda_fail(e != cudaSuccess ? e : e2, "batch graph capture");
+    }
+    e = cudaGraphInstantiate(&c->exec[p], graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_fail(e, "batch graph instantiate");
+  }
+  return FFT3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fft3d_batch_create(int device, fft3d_batch** out) {
+  if (!out) return fft3d::engine_fail(FFT3D_E_PARAM, "neo_fft3d: null output handle");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fft3d::engine_fail(FFT3D_E_NOLIB, "neo_fft3d: no CUDA device");
+  }
+  if (device < 0 || device >= ndev) return fft3d::engine_fail(FFT3D_E_PARAM, "neo_fft3d: invalid device");
+  cudaSetDevice(device);
+  auto* b = new fft3d_batch;
+  b->device = device;
+  cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, device);
+  if (cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    delete b;
+    return fft3d::engine_fail(FFT3D_E_CUDA, "neo_fft3d: stream creation failed");
+  }
+  *out = b;
+  return FFT3D_OK;
+}
+
+void fft3d_batch_destroy(fft3d_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  cudaDeviceSynchronize();
+  b->graphs.clear();
+  if (b->direct_done) cudaEventDestroy(b->direct_done);
+  if (b->h_direct) cudaFreeHost(b->h_direct);
+  if (b->d_direct) cudaFree(b->d_direct);
+  if (b->cap) cudaStreamDestroy(b->cap);
+  delete b;
+}
+
+int fft3d_batch_set_tuning(fft3d_batch* b, int enable) {
+  if (!b) return fft3d::engine_fail(FFT3D_E_PARAM, "neo_fft3d: null handle");
+  std::lock_guard<std::mutex> lk(b->mu);
+  b->tuning = enable ? 1 : 0;
+  return FFT3D_OK;
+}
+
+int fft3d_batch_step(fft3d_batch* b, int count, fft3d_plane* const* planes, const int* n, const void* const* src,
+                     const int* src_stride, void* const* dst, const int* dst_stride, void* stream) {
+  if (!b || count <= 0 || !planes || !n || !src || !src_stride || !dst || !dst_stride)
+    return fft3d::engine_fail(FFT3D_E_PARAM, "neo_fft3d: invalid batch step arguments");
+  std::lock_guard<std::mutex> lk(b->mu);
+  cudaSetDevice(b->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // every plane stays locked until its recorded work is queued
+  std::vector<fft3d_plane*> order(planes, planes + count);
+  std::sort(order.begin(), order.end());
+  if (std::adjacent_find(order.begin(), order.end()) != order.end())
+    return fft3d::engine_fail(FFT3D_E_PARAM, "neo_fft3d: a plane appears twice in one batch step");
+  for (auto* P : order) {
+    if (!P) return fft3d::engine_fail(FFT3D_E_PARAM, "neo_fft3d: null plane in batch step");
+    if (fft3d::plane_device(P) != b->device)
+      return fft3d::engine_fail(FFT3D_E_PARAM, "neo_fft3d: batch planes must live on the batch's device");
+    const std::string why = fft3d::plane_batchable(P);
+    if (!why.empty()) return fft3d::engine_fail(FFT3D_E_UNSUPPORTED, "neo_fft3d: " + why);
+  }
+  std::vector<std::unique_lock<std::mutex>> locks;
+  for (auto* P : order) locks.emplace_back(fft3d::plane_mutex(P));
+  Deferred d;
+  for (int i = 0; i < count; i++) {
+    int rc = fft3d::plane_plan(planes[i], n[i], src + 5 * i, src_stride + 5 * i, dst[i], dst_stride[i], s, &d);
+    if (rc) return rc;
+  }
+  cudaSetDevice(b->device);
+  Plan plan;
+  build_groups(d, plan);
+  b->stats[0] += 1;
+  b->stats[4] = (double)plan.groups.size();
+  fft3d::count_launches(plan.groups.size());
+  Tune& t = b->tunes[plan.sig];
+  if (t.ms.empty()) {
+    t.ms.assign(plan.groups.size(), std::vector<float>(kNumCand, 0.f));
+    b->stats[5] += 1;
+    if (!b->tuning) {
+      t.done = true;
+      t.best.assign(plan.groups.size(), Sched{64, 0});
+    }
+  }
+  if (!t.done) {
+    // tuning step: candidate t.next for every group, each launch timed
+    for (auto& g : plan.groups) g.sched = kCandidates[t.next];
+    set_grids(b, plan);
+    std::vector<cudaEvent_t> ev(2 * plan.groups.size());
+    for (auto& e : ev) cudaEventCreate(&e);
+    int rc = run_direct(b, plan, d, s, &ev);
+    if (rc == FFT3D_OK) {
+      cudaError_t e = cudaEventSynchronize(ev.back());
+      if (e != cudaSuccess) rc = cuda_fail(e, "batch tuning");
+    }
+    if (rc == FFT3D_OK)
+      for (size_t gi = 0; gi < plan.groups.size(); gi++) cudaEventElapsedTime(&t.ms[gi][t.next], ev[2 * gi], ev[2 * gi + 1]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (rc) return rc;
+    b->stats[2] += 1;
+    if (++t.next == kNumCand) {
+      t.best.resize(plan.groups.size());
+      for (size_t gi = 0; gi < plan.groups.size(); gi++) {
+        const auto& m = t.ms[gi];
+        t.best[gi] = kCandidates[std::min_element(m.begin(), m.end()) - m.begin()];
+      }
+      t.done = true;
+    }
+    return FFT3D_OK;
+  }
+  for (size_t gi = 0; gi < plan.groups.size(); gi++) plan.groups[gi].sched = t.best[gi];
+  set_grids(b, plan);
+  auto& slot = b->graphs[plan.sig];
+  if (!slot) {
+    slot.reset(new Captured);
+    int rc = capture(b, plan, slot.get());
+    if (rc) {
+      slot.reset();
+      b->graphs.erase(plan.sig);
+      return rc;
+    }
+  }
+  Captured* c = slot.get();
+  const int p = c->parity;
+  if (c->used[p]) CK(cudaEventSynchronize(c->done[p]), "batch graph staging");
+  write_args(d, plan, static_cast<char*>(c->h_stage[p]));
+  CK(cudaGraphLaunch(c->exec[p], s), "batch graph launch");
+  CK(cudaEventRecord(c->done[p], s), "batch graph event");
+  c->used[p] = true;
+  c->parity ^= 1;
+  b->stats[1] += 1;
+  return FFT3D_OK;
+}
+
+int fft3d_batch_stats(fft3d_batch* b, double out[8]) {
+  if (!b || !out) return fft3d::engine_fail(FFT3D_E_PARAM, "neo_fft3d: null argument");
+  std::lock_guard<std::mutex> lk(b->mu);
+  std::copy(b->stats, b->stats + 8, out);
+  return FFT3D_OK;
+}
+
+}  // extern "C"

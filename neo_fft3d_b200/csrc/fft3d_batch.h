@@ -1,0 +1,41 @@
+// Engine-side interface of the batched multi-plane scheduler (fft3d_batch.cu).
+#pragma once
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "fft3d_b200.h"
+#include "fft3d_kernels.cuh"
+
+namespace fft3d {
+
+// Launches and device copies of one output frame of one plane, recorded in
+// issue order by phase instead of being issued.
+struct Deferred {
+  struct Fwd { ForwardArgs a; int bytes; };
+  struct Inv { InverseArgs a; int mode; };
+  struct Ola { OlaArgs a; int bytes; };
+  struct Copy { void* dst; size_t dpitch; const void* src; size_t spitch; size_t width; size_t height; };
+  std::vector<Fwd> fwd;
+  std::vector<Inv> inv;
+  std::vector<Ola> ola;
+  std::vector<Copy> copies;  // device-to-device, before the overlap-add phase
+};
+
+// Runs plane P's per-frame control for output frame n (device buffers) with
+// every launch and copy recorded in d; the spectrum-ring bookkeeping is done
+// as if they had been issued. The caller holds plane_mutex(P) until the
+// recorded work is queued.
+int plane_plan(fft3d_plane* P, int n, const void* const src[5], const int stride[5], void* dst, int dst_stride,
+               cudaStream_t st, Deferred* d);
+std::mutex& plane_mutex(fft3d_plane* P);
+int plane_device(const fft3d_plane* P);
+// Empty when the scheduler can take the plane, else the reason.
+std::string plane_batchable(const fft3d_plane* P);
+void count_launches(uint64_t n);
+int engine_fail(int code, const std::string& msg);
+
+}  // namespace fft3d

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include "fft3d_b200.h"
+#include "fft3d_batch.h"
 #include "fft3d_kernels.cuh"
 #include "fft3d_psd.h"
 
@@ -25,6 +26,9 @@ namespace {
 
 thread_local std::string g_err;
 std::atomic<uint64_t> g_launches{0};
+// When set, launches and device copies of run_filter are recorded here
+// instead of issued (the batched scheduler, fft3d_batch.cu).
+thread_local fft3d::Deferred* g_defer = nullptr;
 std::mutex g_dev_lock;
 std::vector<int> g_tw_ready;  // devices whose twiddle tables are uploaded
 
@@ -99,7 +103,8 @@ struct fft3d_plane {
   //            (k_forward_tc, 32x32 blocks; other sizes fall back to k_forward)
   int path = 1;  // 0 split, 1 unfused, 2 fused, 3 tc
   uint8_t* d_tc = nullptr;  // tensor-core DFT tables (path 3)
-  int* d_err = nullptr;     // device error flag of the tensor-core kernels
+  int* d_err = nullptr;     // device error flag (tensor-core waits: bit 0, bulk-copy waits: bit 1)
+  int bulk = 0;             // bulk-staged filter/inverse kernel (NEO_FFT3D_INV = regs | bulk)
   float2* d_filt = nullptr;
   // learned noise PSD (fft3d_plane_set_psd): model, per-block noise power, scratch
   fft3d_psd* psd_model = nullptr;
@@ -137,7 +142,7 @@ struct TimeScope {
   cudaStream_t st;
   cudaEvent_t a = nullptr;
   TimeScope(fft3d_plane* p, int k, double b, cudaStream_t s) : P(p), kind(k), bytes(b), st(s) {
-    if (P->timing) {
+    if (P->timing && !g_defer) {
       a = take_event(P);
       cudaEventRecord(a, st);
     }
@@ -269,8 +274,10 @@ void free_plane(fft3d_plane* P) {
   delete P;
 }
 
-int upload_pattern(fft3d_plane* P, float* dptr, const std::vector<float>& v) {
-  CK(cudaMemcpyAsync(dptr, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice, P->stream), "pattern upload");
+int upload_pattern(fft3d_plane* P, float* dptr, const std::vector<float>& v, cudaStream_t st) {
+  CK(cudaMemcpyAsync(dptr, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice, st), "pattern upload");
+  // the source is a temporary host vector: the copy must have read it
+  CK(cudaStreamSynchronize(st), "pattern upload");
   return FFT3D_OK;
 }
 
@@ -304,6 +311,10 @@ fft3d::ForwardArgs forward_args(fft3d_plane* P, const void* plane, long long str
 
 int launch_forward(fft3d_plane* P, const void* plane, long long stride, float2* spec, cudaStream_t st) {
   fft3d::ForwardArgs a = forward_args(P, plane, stride, spec);
+  if (g_defer) {
+    g_defer->fwd.push_back({a, P->bytes});
+    return FFT3D_OK;
+  }
   TimeScope ts(P, K_FORWARD, (double)P->g.W * P->g.H * P->bytes + (double)P->spec_elems() * sizeof(float2), st);
   if (P->d_tc) {
     CK(fft3d::launch_forward_tc(a, P->d_tc, P->d_err, P->bytes, st), "tensor-core forward kernel");
@@ -342,6 +353,11 @@ int spectrum_slot(fft3d_plane* P, int m, int lo, int hi, const void* plane, int 
 
 int copy_plane(fft3d_plane* P, void* dst, int dstride, const void* src, int sstride, cudaMemcpyKind kind,
                cudaStream_t st) {
+  if (g_defer && kind == cudaMemcpyDeviceToDevice) {
+    g_defer->copies.push_back({dst, (size_t)dstride, src, (size_t)sstride, (size_t)P->d.width * P->bytes,
+                               (size_t)P->d.height});
+    return FFT3D_OK;
+  }
   CK(cudaMemcpy2DAsync(dst, dstride, src, sstride, (size_t)P->d.width * P->bytes, P->d.height, kind, st),
      "plane copy");
   return FFT3D_OK;
@@ -368,7 +384,7 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
   if (bt > 0 && btcur > 1 && P->pattern && !P->pattern3d_init) {  // :625-630
     std::vector<float> p3(P->h_pattern2d.size());
     for (size_t i = 0; i < p3.size(); i++) p3[i] = P->h_pattern2d[i] * (float)btcur;
-    int rc = upload_pattern(P, P->d_pattern3d, p3);
+    int rc = upload_pattern(P, P->d_pattern3d, p3, st);
     if (rc) return rc;
     P->pattern3d_init = true;
   }
@@ -439,6 +455,8 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
   ia.kal_covar = P->d_cov;
   ia.kal_covarp = P->d_covp;
   ia.tdom = P->d_tdom;
+  ia.err = P->d_err;
+  ia.bulk = (P->path == 1 || P->path == 3) ? P->bulk : 0;
   ia.reverse = (int)(P->frames_done++ & 1);
   {
     const double S = (double)P->spec_elems() * sizeof(float2);
@@ -465,6 +483,8 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
       // reads: the filtered spectrum; writes: the time-domain blocks
       TimeScope ts(P, K_INVERSE, S + T, st);
       CK(fft3d::launch_filter_inverse(sa, fft3d::MODE_SHARPEN_ONLY, st), "sharpen/inverse kernel");
+    } else if (g_defer) {
+      g_defer->inv.push_back({ia, mode});
     } else {
       // reads: the spectra of the window (+ Kalman state); writes: the time-domain blocks
       TimeScope ts(P, K_INVERSE, (to - from + 1) * S + state + T, st);
@@ -475,7 +495,7 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
     news->frame = newest;
     news->stamp = ++P->clock;
   }
-  g_launches++;
+  if (!g_defer) g_launches++;
   // output: the crop borders come from the source frame (src/fft3d.hpp:292-352)
   const bool crop = ep.l > 0 || ep.t > 0 || ep.r > 0 || ep.b > 0;
   void* odst = dst;
@@ -505,11 +525,13 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
   oa.rounder = ints ? 0.5f : 0.f;
   oa.base = (ints && P->d.is_chroma) ? (float)(1 << (P->d.bits - 1)) : 0.f;
   oa.maxval = P->bytes == 1 ? 255 : (1 << P->d.bits) - 1;
-  {
+  if (g_defer) {
+    g_defer->ola.push_back({oa, P->bytes});
+  } else {
     TimeScope ts(P, K_OLA, (double)P->g.nblocks * P->g.bh * P->g.bw * 4 + (double)P->g.W * P->g.H * P->bytes, st);
     CK(fft3d::launch_overlap_add(oa, P->bytes, st), "overlap-add kernel");
+    g_launches++;
   }
-  g_launches++;
   if (host) {
     char* hdst = static_cast<char*>(dst) + (size_t)P->t * dst_stride + (size_t)P->l * P->bytes;
     const char* ddst = static_cast<const char*>(P->d_out) + P->t * P->out_pitch + (size_t)P->l * P->bytes;
@@ -520,7 +542,11 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
       if (!flagp) continue;
       int flag = 0;
       CK(cudaMemcpy(&flag, flagp, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
-      if (flag) return fail(FFT3D_E_CUDA, "neo_fft3d: tensor-core MMA completion wait timed out");
+      if (flag) {
+        cudaMemset(flagp, 0, sizeof(int));
+        return fail(FFT3D_E_CUDA, (flag & 2) ? "neo_fft3d: bulk copy completion wait timed out"
+                                             : "neo_fft3d: tensor-core MMA completion wait timed out");
+      }
     }
   }
   return FFT3D_OK;
@@ -530,6 +556,29 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
 
 namespace fft3d {
 void set_last_error(const std::string& msg) { g_err = msg; }
+
+int plane_plan(fft3d_plane* P, int n, const void* const src[5], const int stride[5], void* dst, int dst_stride,
+               cudaStream_t st, Deferred* d) {
+  cudaSetDevice(P->device);
+  g_defer = d;
+  const int rc = run_filter(P, n, src, stride, dst, dst_stride, false, st);
+  g_defer = nullptr;
+  return rc;
+}
+
+std::mutex& plane_mutex(fft3d_plane* P) { return P->mu; }
+int plane_device(const fft3d_plane* P) { return P->device; }
+
+std::string plane_batchable(const fft3d_plane* P) {
+  if (P->path != 1) return "the batched scheduler runs the default (unfused) path";
+  if (P->d_tc) return "tensor-core planes are not batched";
+  if (P->psd_model) return "planes with a learned noise PSD are not batched";
+  if (P->bulk) return "the bulk-staged inverse is not batched";
+  return "";
+}
+
+void count_launches(uint64_t n) { g_launches += n; }
+int engine_fail(int code, const std::string& msg) { return fail(code, msg); }
 }  // namespace fft3d
 
 extern "C" {
@@ -563,6 +612,9 @@ int fft3d_plane_create(const fft3d_params* p, const fft3d_plane_desc* d, int dev
     const char* f = std::getenv("NEO_FFT3D_PATH");
     std::string v = f ? f : "unfused";
     P->path = v == "fused" ? 2 : (v == "split" ? 0 : (v == "tc" ? 3 : 1));
+    // filter/inverse kernel of the unfused and tc paths: register-pipelined (default) or bulk-staged
+    const char* iv = std::getenv("NEO_FFT3D_INV");
+    P->bulk = iv && std::string(iv) == "bulk";
   }
   fft3d_params& ep = P->ep;
   if (d->bits < 8 || (d->bits > 16 && d->bits != 32)) { delete P; return fail(FFT3D_E_PARAM, "neo_fft3d: unsupported bit depth"); }
@@ -714,12 +766,13 @@ int fft3d_plane_create(const fft3d_params* p, const fft3d_plane_desc* d, int dev
   if (P->path == 3 && ep.bw == 32 && ep.bh == 32) {
     std::vector<uint8_t> tc(fft3d::forward_tc_table_bytes());
     fft3d::forward_tc_tables(wx.data(), wy.data(), tc.data());
-    if (cudaMalloc(&P->d_tc, tc.size()) != cudaSuccess || cudaMalloc(&P->d_err, sizeof(int)) != cudaSuccess)
+    if (cudaMalloc(&P->d_tc, tc.size()) != cudaSuccess)
       return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (tensor-core tables)"));
-    if (cudaMemcpy(P->d_tc, tc.data(), tc.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemset(P->d_err, 0, sizeof(int)) != cudaSuccess)
+    if (cudaMemcpy(P->d_tc, tc.data(), tc.size(), cudaMemcpyHostToDevice) != cudaSuccess)
       return bail(fail(FFT3D_E_CUDA, "neo_fft3d: tensor-core table upload failed"));
   }
+  if (cudaMalloc(&P->d_err, sizeof(int)) != cudaSuccess || cudaMemset(P->d_err, 0, sizeof(int)) != cudaSuccess)
+    return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (error flag)"));
   if (P->path == 0 && cudaMalloc(&P->d_filt, P->spec_elems() * sizeof(float2)) != cudaSuccess)
     return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (filtered spectrum)"));
   if (cudaMalloc(&P->d_tdom, (size_t)g.nblocks * bh * bw * sizeof(float)) != cudaSuccess)
@@ -815,7 +868,7 @@ int fft3d_plane_set_pattern_frame(fft3d_plane* P, const void* src, int stride) {
      "spectrum download");
   CK(cudaStreamSynchronize(P->stream), "synchronize");
   estimate_pattern(P, spec);
-  rc = upload_pattern(P, P->d_pattern2d, P->h_pattern2d);
+  rc = upload_pattern(P, P->d_pattern2d, P->h_pattern2d, P->stream);
   if (rc) return rc;
   CK(cudaStreamSynchronize(P->stream), "synchronize");
   P->pattern_set = true;

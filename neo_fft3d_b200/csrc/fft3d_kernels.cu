@@ -41,10 +41,8 @@ __device__ __forceinline__ void store_sample<float>(float* p, float v, int) {
 // blocks covering it, weighted with the synthesis windows and the FFT
 // normalisation in the association order of src/buffer.cpp:399-559.
 template <typename T>
-__global__ void k_overlap_add(OlaArgs a) {
+__device__ __forceinline__ void overlap_add_px(const OlaArgs& a, int x0, int k) {
   const Geom& g = a.g;
-  const int x0 = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = blockIdx.y * blockDim.y + threadIdx.y;
   if (x0 >= g.W || k >= g.H) return;
   const int Y = g.sy + k, X = g.sx + x0;
   const int by = Y / g.sy, y = Y - by * g.sy;
@@ -75,6 +73,26 @@ __global__ void k_overlap_add(OlaArgs a) {
   }
   T* row = reinterpret_cast<T*>(static_cast<char*>(a.dst) + (long long)field_row(k, g.H, g.interlaced) * a.dst_stride);
   store_sample<T>(row + x0, v, a.maxval);
+}
+
+constexpr int kOlaTx = 32, kOlaTy = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(kOlaTx * kOlaTy) k_overlap_add(OlaArgs a) {
+  overlap_add_px<T>(a, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y);
+}
+
+// Batched overlap-add: work item = (plane, 32x8 tile in row-major tile order).
+template <typename T>
+__global__ void __launch_bounds__(kOlaTx * kOlaTy) k_overlap_add_batch(const OlaArgs* __restrict__ args,
+                                                                      const int2* __restrict__ items, int nitems) {
+  for (int i = blockIdx.x; i < nitems; i += gridDim.x) {
+    const int2 it = items[i];
+    const OlaArgs& a = args[it.x];
+    const int tx = (a.g.W + kOlaTx - 1) / kOlaTx;
+    const int ty = it.y / tx, t = it.y - ty * tx;
+    overlap_add_px<T>(a, t * kOlaTx + threadIdx.x, ty * kOlaTy + threadIdx.y);
+  }
 }
 
 }  // namespace
@@ -141,9 +159,73 @@ cudaError_t launch_fused(const FusedArgs& a, int mode, int bytes, cudaStream_t s
   return e ? e->fused(a, mode, bytes, s) : cudaErrorInvalidValue;
 }
 
+cudaError_t launch_forward_batch(int bw, int bh, const BatchLaunch& l, int bytes, cudaStream_t s) {
+  const SizeEntry* e = find_size(bw, bh);
+  return e ? e->fwd_batch(l, bytes, s) : cudaErrorInvalidValue;
+}
+
+cudaError_t launch_filter_inverse_batch(int bw, int bh, const BatchLaunch& l, int mode, cudaStream_t s) {
+  const SizeEntry* e = find_size(bw, bh);
+  return e ? e->inv_batch(l, mode, s) : cudaErrorInvalidValue;
+}
+
+cudaError_t launch_overlap_add_batch(const BatchLaunch& l, int bytes, cudaStream_t s) {
+  dim3 block(kOlaTx, kOlaTy);
+  const auto* args = static_cast<const OlaArgs*>(l.args);
+  if (bytes == 1) k_overlap_add_batch<uint8_t><<<l.grid, block, 0, s>>>(args, l.items, l.nitems);
+  else if (bytes == 2) k_overlap_add_batch<uint16_t><<<l.grid, block, 0, s>>>(args, l.items, l.nitems);
+  else k_overlap_add_batch<float><<<l.grid, block, 0, s>>>(args, l.items, l.nitems);
+  return cudaGetLastError();
+}
+
+// Batched plane copies: work item = (copy, row); 16-byte moves when both
+// rows are 16-byte aligned, bytes otherwise.
+__global__ void __launch_bounds__(256) k_copy_batch(const CopyArgs* __restrict__ args, const int2* __restrict__ items,
+                                                    int nitems) {
+  for (int i = blockIdx.x; i < nitems; i += gridDim.x) {
+    const int2 it = items[i];
+    const CopyArgs& c = args[it.x];
+    const char* s = static_cast<const char*>(c.src) + (long long)it.y * c.spitch;
+    char* d = static_cast<char*>(c.dst) + (long long)it.y * c.dpitch;
+    if ((((uintptr_t)s | (uintptr_t)d) & 15) == 0) {
+      const long long n16 = c.width / 16;
+      for (long long x = threadIdx.x; x < n16; x += blockDim.x)
+        reinterpret_cast<uint4*>(d)[x] = reinterpret_cast<const uint4*>(s)[x];
+      for (long long x = n16 * 16 + threadIdx.x; x < c.width; x += blockDim.x) d[x] = s[x];
+    } else {
+      for (long long x = threadIdx.x; x < c.width; x += blockDim.x) d[x] = s[x];
+    }
+  }
+}
+
+cudaError_t launch_copy_batch(const BatchLaunch& l, cudaStream_t s) {
+  k_copy_batch<<<l.grid, 256, 0, s>>>(static_cast<const CopyArgs*>(l.args), l.items, l.nitems);
+  return cudaGetLastError();
+}
+
+int batch_items_forward(const Geom& g) {
+  const SizeEntry* e = find_size(g.bw, g.bh);
+  return e ? e->ctas(g.nblocks) : 0;
+}
+
+int batch_items_overlap_add(const Geom& g) {
+  return ((g.W + kOlaTx - 1) / kOlaTx) * ((g.H + kOlaTy - 1) / kOlaTy);
+}
+
+int batch_occupancy(int bw, int bh, int which, int mode_or_bytes) {
+  if (which == 3) return 8;  // plane copies
+  if (which == 2) {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_overlap_add_batch<uint8_t>, kOlaTx * kOlaTy, 0);
+    return n > 0 ? n : 1;
+  }
+  const SizeEntry* e = find_size(bw, bh);
+  return e ? e->occupancy(which, mode_or_bytes) : 1;
+}
+
 cudaError_t launch_overlap_add(const OlaArgs& a, int bytes, cudaStream_t s) {
-  dim3 block(32, 8);
-  dim3 grid((a.g.W + 31) / 32, (a.g.H + 7) / 8);
+  dim3 block(kOlaTx, kOlaTy);
+  dim3 grid((a.g.W + kOlaTx - 1) / kOlaTx, (a.g.H + kOlaTy - 1) / kOlaTy);
   if (bytes == 1) k_overlap_add<uint8_t><<<grid, block, 0, s>>>(a);
   else if (bytes == 2) k_overlap_add<uint16_t><<<grid, block, 0, s>>>(a);
   else k_overlap_add<float><<<grid, block, 0, s>>>(a);

@@ -87,6 +87,8 @@ struct InverseArgs {
                           // [blocks][bh*nh] when psd_per_block, else [bh*nh]
   float psd_scale;        // btcur for Wiener 3D (pattern3d = bt x pattern2d), else 1
   int psd_per_block;
+  int* err;               // device error flag (bit 1: a bounded bulk-copy wait ran out)
+  int bulk;               // use the bulk-staged filter/inverse kernel where it applies
   int reverse;            // walk the blocks from the end (alternated per frame so
                           // that the blocks read last stay in L2 for the next frame)
 };
@@ -111,10 +113,37 @@ struct OlaArgs {
   int maxval;             // (1 << bits) - 1
 };
 
+// One batched launch: `nitems` work items (plane index into `args`, CTA of
+// that plane) walked by a grid of `grid` CTAs; args/items in device memory.
+struct BatchLaunch {
+  const void* args;
+  const int2* items;
+  int nitems;
+  int grid;
+};
+
+// One device-to-device plane copy of a batch (crop borders, Kalman frame 0).
+struct CopyArgs {
+  void* dst;
+  long long dpitch;
+  const void* src;
+  long long spitch;
+  long long width;  // bytes per row
+  int height;
+};
+
 // Host-side launchers (fft3d_kernels.cu). They return cudaGetLastError().
 cudaError_t launch_forward(const ForwardArgs& a, int bytes_per_sample, cudaStream_t s);
 cudaError_t launch_filter_inverse(const InverseArgs& a, int mode, cudaStream_t s);
 cudaError_t launch_overlap_add(const OlaArgs& a, int bytes_per_sample, cudaStream_t s);
+// Batched forms (work items as in BatchLaunch); OLA items are 32x8-pixel tiles.
+cudaError_t launch_forward_batch(int bw, int bh, const BatchLaunch& l, int bytes_per_sample, cudaStream_t s);
+cudaError_t launch_filter_inverse_batch(int bw, int bh, const BatchLaunch& l, int mode, cudaStream_t s);
+cudaError_t launch_overlap_add_batch(const BatchLaunch& l, int bytes_per_sample, cudaStream_t s);
+cudaError_t launch_copy_batch(const BatchLaunch& l, cudaStream_t s);  // items: (copy, row)
+int batch_items_forward(const Geom& g);     // forward / filter-inverse work items of a plane
+int batch_items_overlap_add(const Geom& g);  // overlap-add work items (tiles) of a plane
+int batch_occupancy(int bw, int bh, int which, int mode_or_bytes);  // which: 0 fwd, 1 inv, 2 ola
 // Streaming filter of all bins (Wiener 2D/3D, Kalman) into F; the sharpen pass
 // and the inverse follow with launch_filter_inverse(MODE_SHARPEN_ONLY) on F.
 cudaError_t launch_filter_bins(const InverseArgs& a, float2* F, int mode, cudaStream_t s);

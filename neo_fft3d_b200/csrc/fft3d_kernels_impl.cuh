@@ -2,6 +2,7 @@
 // Included by the per-size translation units kern_*.cu, which instantiate the
 // block sizes they own and register them in the size table (kern_registry.h).
 #pragma once
+#include <algorithm>
 #include <cmath>
 
 #include "fft3d_kernels.cuh"
@@ -207,13 +208,13 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // One warp transforms blocks_per_warp<BW>() consecutive blocks (rows, then
 // columns, then a coalesced 16-byte copy-out of the contiguous spectra).
 template <int BW, int BH, typename T>
-__global__ void __launch_bounds__(kWarps * 32) k_forward(ForwardArgs a) {
+__device__ __forceinline__ void forward_cta(const ForwardArgs& a, int cta) {
   constexpr int NH = BW / 2 + 1, HC = BW / 2, NBW = blocks_per_warp<BW>(), BINS = BH * NH;
   extern __shared__ float2 smem2[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float2* S = smem2 + warp * NBW * BINS;
   const Geom& g = a.g;
-  const int blk0 = (blockIdx.x * kWarps + warp) * NBW;
+  const int blk0 = (cta * kWarps + warp) * NBW;
   if (blk0 >= g.nblocks) return;
   for (int t = lane; t < NBW * BH; t += 32) {
     const int b = t / BH, y = t - b * BH;
@@ -229,6 +230,23 @@ __global__ void __launch_bounds__(kWarps * 32) k_forward(ForwardArgs a) {
   float4* dst = reinterpret_cast<float4*>(a.spec + (size_t)blk0 * BINS);
   const float4* src = reinterpret_cast<const float4*>(S);
   for (int i = lane; i < nvalid * BINS / 2; i += 32) dst[i] = src[i];
+  __syncwarp();  // S is reused by the warp's next work item
+}
+
+template <int BW, int BH, typename T>
+__global__ void __launch_bounds__(kWarps * 32) k_forward(ForwardArgs a) {
+  forward_cta<BW, BH, T>(a, blockIdx.x);
+}
+
+// Batched forward: work item i = (plane, CTA of that plane); the grid walks
+// the items (persistent when the grid is smaller than the item count).
+template <int BW, int BH, typename T>
+__global__ void __launch_bounds__(kWarps * 32) k_forward_batch(const ForwardArgs* __restrict__ args,
+                                                              const int2* __restrict__ items, int nitems) {
+  for (int i = blockIdx.x; i < nitems; i += gridDim.x) {
+    const int2 it = items[i];
+    forward_cta<BW, BH, T>(args[it.x], it.y);
+  }
 }
 
 // ---------------------------------------------------------------- filters
@@ -465,15 +483,20 @@ __global__ void __launch_bounds__(256) k_filter_bins(InverseArgs a, float2* F, i
 //  B. one column per lane: inverse complex DFT along y (DC and Nyquist columns
 //     together: both are Hermitian, so their inverses are real);
 //  C. one row per lane: c2r along x, 16-byte stores of the time-domain rows.
+template <int BW, int BH>
+__host__ __device__ constexpr int fft_ctas(int nblocks) {
+  return (nblocks + kWarps * blocks_per_warp<BW>() - 1) / (kWarps * blocks_per_warp<BW>());
+}
+
 template <int BW, int BH, int MODE>
-__global__ void __launch_bounds__(kWarps * 32) k_filter_inverse(InverseArgs a) {
+__device__ __forceinline__ void filter_inverse_cta(const InverseArgs& a, int vcta) {
   constexpr int NH = BW / 2 + 1, HC = BW / 2, NBW = blocks_per_warp<BW>(), BINS = BH * NH;
   constexpr int PER = (BINS + 31) / 32;
   extern __shared__ float2 smem2[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float2* S = smem2 + warp * NBW * BINS;
   const Geom& g = a.g;
-  const int cta = a.reverse ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
+  const int cta = a.reverse ? fft_ctas<BW, BH>(g.nblocks) - 1 - vcta : vcta;
   const int blk0 = (cta * kWarps + warp) * NBW;
   if (blk0 >= g.nblocks) return;
   const float gs0 = __ldg(&a.t.grid[0].x);
@@ -529,6 +552,133 @@ __global__ void __launch_bounds__(kWarps * 32) k_filter_inverse(InverseArgs a) {
   __syncwarp();
   for (int b = 0; b < NBW && blk0 + b < g.nblocks; b++)
     store_tdom<BW, BH>(S + b * BINS, a.tdom + (size_t)(blk0 + b) * BH * BW, lane);
+  __syncwarp();  // S is reused by the warp's next work item
+}
+
+template <int BW, int BH, int MODE>
+__global__ void __launch_bounds__(kWarps * 32) k_filter_inverse(InverseArgs a) {
+  filter_inverse_cta<BW, BH, MODE>(a, blockIdx.x);
+}
+
+template <int BW, int BH, int MODE>
+__global__ void __launch_bounds__(kWarps * 32) k_filter_inverse_batch(const InverseArgs* __restrict__ args,
+                                                                     const int2* __restrict__ items, int nitems) {
+  for (int i = blockIdx.x; i < nitems; i += gridDim.x) {
+    const int2 it = items[i];
+    filter_inverse_cta<BW, BH, MODE>(args[it.x], it.y);
+  }
+}
+
+// ---------------------------------------------------------------- inverse (bulk-staged)
+
+constexpr int kBulkWarps = 4;
+constexpr int kBulkSpin = 1 << 22;  // bounded mbarrier wait (then error flag 2)
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ bool bulk_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done = 0;
+  for (int it = 0; it < kBulkSpin && !done; it++)
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+  return done != 0;
+}
+
+template <int BW, int BH, int MODE>
+__host__ __device__ constexpr int bulk_warp_bytes() {
+  return (win_hi<MODE>() - win_lo<MODE>() + 2) * BH * (BW / 2 + 1) * 8;
+}
+
+// Filter + inverse with the window's spectra fetched by bulk copies: each
+// warp walks its blocks (block = warp index + k * all warps, or mirrored for
+// the reverse order) with a stage holding the block's window spectra (one
+// contiguous BH x NH run per frame, one cp.async.bulk each, completing on
+// the warp's mbarrier). The filter reads the stage and writes the block's
+// filtered spectrum to S; lane 0 then refills the stage with the next
+// block's spectra, which land while the warp runs the inverse transform of S
+// and stores the time-domain block. Wiener and sharpen-only modes.
+template <int BW, int BH, int MODE>
+__global__ void __launch_bounds__(kBulkWarps * 32) k_filter_inverse_bulk(InverseArgs a) {
+  constexpr int NH = BW / 2 + 1, HC = BW / 2, BINS = BH * NH, PER = (BINS + 31) / 32;
+  constexpr int LO = win_lo<MODE>(), NW = win_hi<MODE>() - win_lo<MODE>() + 1;
+  constexpr uint32_t SPEC_BYTES = BINS * 8;
+  static_assert(SPEC_BYTES % 16 == 0, "bulk copies move multiples of 16 bytes");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* stage = reinterpret_cast<float2*>(smem_raw + 128 + (size_t)warp * bulk_warp_bytes<BW, BH, MODE>());
+  float2* S = stage + NW * BINS;
+  uint64_t* bar = bars + warp;
+  const Geom& g = a.g;
+  const int nwarps = gridDim.x * kBulkWarps;
+  const int first = blockIdx.x * kBulkWarps + warp;
+  if (first >= g.nblocks) return;
+  auto block_of = [&](int idx) { return a.reverse ? g.nblocks - 1 - idx : idx; };
+  auto fetch = [&](int blk) {  // lane 0
+    const size_t off = (size_t)blk * BINS;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(NW * SPEC_BYTES)
+                 : "memory");
+#pragma unroll
+    for (int k = 0; k < NW; k++)
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              smem_addr(stage + k * BINS)),
+          "l"(a.in[LO + k] + off), "r"(SPEC_BYTES), "r"(smem_addr(bar))
+          : "memory");
+  };
+  if (lane == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    fetch(block_of(first));
+  }
+  __syncwarp();
+  const float gs0 = __ldg(&a.t.grid[0].x);
+  uint32_t phase = 0;
+  for (int idx = first; idx < g.nblocks; idx += nwarps) {
+    const int blk = block_of(idx);
+    if (!__all_sync(0xffffffffu, bulk_wait(bar, phase))) {
+      // the copies never completed: flag it, give them one more bounded wait
+      // (they target this warp's shared memory), and stop
+      if (lane == 0) atomicOr(a.err, 2);
+      bulk_wait(bar, phase);
+      return;
+    }
+    phase ^= 1;
+    const size_t off = (size_t)blk * BINS;
+    const float gf = (MODE >= 1) ? a.c.degrid * stage[(2 - LO) * BINS].x / gs0 : 0.f;
+    float gsh = 0.f;
+#pragma unroll 1
+    for (int j = 0; j < PER; j++) {
+      const int i = lane + 32 * j;
+      float2 v = make_float2(0.f, 0.f);
+      if (i < BINS) {
+        float2 w[5];
+#pragma unroll
+        for (int k = 0; k < 5; k++)
+          w[k] = (k >= LO && k < LO + NW) ? stage[(k - LO) * BINS + i] : make_float2(0.f, 0.f);
+        v = filter_vals<MODE>(a, w, off, i, gf, true);
+      }
+      if (a.c.do_sharpen) {
+        if (j == 0) gsh = a.c.degrid * __shfl_sync(0xffffffffu, v.x, 0) / gs0;
+        if (i < BINS) v = sharpen_bin(a, v, i, gsh);
+      }
+      if (i < BINS) S[i] = v;
+    }
+    __syncwarp();
+    if (lane == 0 && idx + nwarps < g.nblocks) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      fetch(block_of(idx + nwarps));
+    }
+    for (int c = lane; c < HC; c += 32) inv_col<BW, BH>(S, c);
+    __syncwarp();
+    for (int y = lane; y < BH; y += 32) inv_row_inplace<BW, BH>(S, y);
+    __syncwarp();
+    store_tdom<BW, BH>(S, a.tdom + (size_t)blk * BH * BW, lane);
+    __syncwarp();
+  }
 }
 
 // ---------------------------------------------------------------- fused
@@ -613,8 +763,79 @@ __global__ void __launch_bounds__(kFusedWarps * 32) k_fused(FusedArgs A) {
 
 template <int BW, int BH>
 int fft_grid(int nblocks) {
-  const int per_cta = kWarps * blocks_per_warp<BW>();
-  return (nblocks + per_cta - 1) / per_cta;
+  return fft_ctas<BW, BH>(nblocks);
+}
+
+// Batched launches of one kernel variant over many planes (see k_forward_batch).
+template <int BW, int BH>
+cudaError_t fwd_batch(const BatchLaunch& l, int bytes, cudaStream_t s) {
+  const int smem = kWarps * fft_smem_bytes<BW, BH>();
+  const auto* args = static_cast<const ForwardArgs*>(l.args);
+  cudaError_t e = cudaSuccess;
+  if (bytes == 1) {
+    e = cudaFuncSetAttribute(k_forward_batch<BW, BH, uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) k_forward_batch<BW, BH, uint8_t><<<l.grid, kWarps * 32, smem, s>>>(args, l.items, l.nitems);
+  } else if (bytes == 2) {
+    e = cudaFuncSetAttribute(k_forward_batch<BW, BH, uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) k_forward_batch<BW, BH, uint16_t><<<l.grid, kWarps * 32, smem, s>>>(args, l.items, l.nitems);
+  } else {
+    e = cudaFuncSetAttribute(k_forward_batch<BW, BH, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) k_forward_batch<BW, BH, float><<<l.grid, kWarps * 32, smem, s>>>(args, l.items, l.nitems);
+  }
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+template <int BW, int BH, int MODE>
+cudaError_t inv_batch_mode(const BatchLaunch& l, cudaStream_t s) {
+  const int smem = kWarps * fft_smem_bytes<BW, BH>();
+  cudaError_t e = cudaFuncSetAttribute(k_filter_inverse_batch<BW, BH, MODE>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  k_filter_inverse_batch<BW, BH, MODE><<<l.grid, kWarps * 32, smem, s>>>(static_cast<const InverseArgs*>(l.args),
+                                                                         l.items, l.nitems);
+  return cudaGetLastError();
+}
+
+template <int BW, int BH>
+cudaError_t inv_batch(const BatchLaunch& l, int mode, cudaStream_t s) {
+  switch (mode) {
+    case MODE_SHARPEN_ONLY: return inv_batch_mode<BW, BH, MODE_SHARPEN_ONLY>(l, s);
+    case MODE_KALMAN: return inv_batch_mode<BW, BH, MODE_KALMAN>(l, s);
+    case 1: return inv_batch_mode<BW, BH, 1>(l, s);
+    case 2: return inv_batch_mode<BW, BH, 2>(l, s);
+    case 3: return inv_batch_mode<BW, BH, 3>(l, s);
+    case 4: return inv_batch_mode<BW, BH, 4>(l, s);
+    case 5: return inv_batch_mode<BW, BH, 5>(l, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+// CTAs of one plane's unbatched launch (the work items per plane of a batch)
+template <int BW, int BH>
+int ctas_per_plane(int nblocks) {
+  return fft_ctas<BW, BH>(nblocks);
+}
+
+// Occupancy (resident CTAs per SM) of the batched kernels.
+template <int BW, int BH>
+int occupancy_of(int which, int mode_or_bytes) {
+  const int smem = kWarps * fft_smem_bytes<BW, BH>();
+  int n = 0;
+  if (which == 0) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_forward_batch<BW, BH, uint8_t>, kWarps * 32, smem);
+  } else {
+    switch (mode_or_bytes) {
+      case MODE_KALMAN:
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_filter_inverse_batch<BW, BH, MODE_KALMAN>, kWarps * 32, smem);
+        break;
+      case 5:
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_filter_inverse_batch<BW, BH, 5>, kWarps * 32, smem);
+        break;
+      default:
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_filter_inverse_batch<BW, BH, 3>, kWarps * 32, smem);
+    }
+  }
+  return n > 0 ? n : 1;
 }
 
 template <int BW, int BH>
@@ -637,6 +858,21 @@ cudaError_t fwd_sized(const ForwardArgs& a, int bytes, cudaStream_t s) {
 
 template <int BW, int BH, int MODE>
 cudaError_t inv_mode(const InverseArgs& a, cudaStream_t s) {
+  constexpr int bulk_smem = 128 + kBulkWarps * bulk_warp_bytes<BW, BH, MODE>();
+  if (MODE != MODE_KALMAN && a.bulk && a.err && bulk_smem <= 160 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_filter_inverse_bulk<BW, BH, MODE>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, bulk_smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0, dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_filter_inverse_bulk<BW, BH, MODE>, kBulkWarps * 32,
+                                                  bulk_smem);
+    const int need = (a.g.nblocks + kBulkWarps - 1) / kBulkWarps;
+    const int grid = std::min(need, std::max(1, per_sm) * sms);
+    k_filter_inverse_bulk<BW, BH, MODE><<<grid, kBulkWarps * 32, bulk_smem, s>>>(a);
+    return cudaGetLastError();
+  }
   const int smem = kWarps * fft_smem_bytes<BW, BH>();
   const int grid = fft_grid<BW, BH>(a.g.nblocks);
   cudaError_t e =
@@ -696,8 +932,9 @@ cudaError_t inv_sized(const InverseArgs& a, int mode, cudaStream_t s) {
 }  // namespace
 
 // Registers block size BW x BH of this translation unit in the size table.
-#define FFT3D_REGISTER_SIZE(BW, BH)                                                                  \
-  static const bool fft3d_reg_##BW##x##BH = register_size(                                          \
-      SizeEntry{BW, BH, &fwd_sized<BW, BH>, &inv_sized<BW, BH>, &fused_sized<BW, BH>, &upload_twiddle_table});
+#define FFT3D_REGISTER_SIZE(BW, BH)                                                                     \
+  static const bool fft3d_reg_##BW##x##BH = register_size(                                             \
+      SizeEntry{BW, BH, &fwd_sized<BW, BH>, &inv_sized<BW, BH>, &fused_sized<BW, BH>, &upload_twiddle_table, \
+                &fwd_batch<BW, BH>, &inv_batch<BW, BH>, &ctas_per_plane<BW, BH>, &occupancy_of<BW, BH>});
 
 }  // namespace fft3d

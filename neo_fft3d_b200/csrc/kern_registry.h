@@ -14,6 +14,11 @@ struct SizeEntry {
   cudaError_t (*inv)(const InverseArgs&, int mode, cudaStream_t);
   cudaError_t (*fused)(const FusedArgs&, int mode, int bytes_per_sample, cudaStream_t);
   cudaError_t (*upload)();  // the translation unit's twiddle table, once per device
+  // batched launches over many planes (fft3d_batch.cu)
+  cudaError_t (*fwd_batch)(const BatchLaunch&, int bytes_per_sample, cudaStream_t);
+  cudaError_t (*inv_batch)(const BatchLaunch&, int mode, cudaStream_t);
+  int (*ctas)(int nblocks);                       // work items (CTAs) per plane
+  int (*occupancy)(int which, int mode_or_bytes);  // resident CTAs per SM: 0 forward, 1 filter/inverse
 };
 
 bool register_size(const SizeEntry& e);

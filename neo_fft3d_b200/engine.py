@@ -52,6 +52,12 @@ def lib():
         L.fft3d_plane_set_timing.argtypes = [vp, ci]
         L.fft3d_plane_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         L.fft3d_plane_set_psd.argtypes = [vp, vp, ci, ctypes.c_float]
+        L.fft3d_batch_create.argtypes = [ci, ctypes.POINTER(vp)]
+        L.fft3d_batch_destroy.argtypes = [vp]
+        L.fft3d_batch_set_tuning.argtypes = [vp, ci]
+        L.fft3d_batch_step.argtypes = [vp, ci, ctypes.POINTER(vp), ctypes.POINTER(ci), ctypes.POINTER(vp),
+                                       ctypes.POINTER(ci), ctypes.POINTER(vp), ctypes.POINTER(ci), vp]
+        L.fft3d_batch_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         _lib = L
     return _lib
 
@@ -134,6 +140,46 @@ class PlaneEngine:
     def close(self):
         if getattr(self, "h", None):
             lib().fft3d_plane_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Batched multi-plane scheduler (fft3d_batch_*): one step filters one
+    frame of each of many planes with batched, tuned, graph-captured launches."""
+
+    def __init__(self, device: int = 0, tuning: bool = True):
+        h = ctypes.c_void_p()
+        _check(lib().fft3d_batch_create(device, ctypes.byref(h)))
+        self.h = h
+        _check(lib().fft3d_batch_set_tuning(self.h, 1 if tuning else 0))
+
+    def step(self, items, stream: int = 0):
+        """items: list of (PlaneEngine, n, src_ptrs[5], src_strides[5], dst_ptr, dst_stride)."""
+        k = len(items)
+        planes = (ctypes.c_void_p * k)(*[it[0].h.value for it in items])
+        ns = (ctypes.c_int * k)(*[it[1] for it in items])
+        src = (ctypes.c_void_p * (5 * k))(*[p or None for it in items for p in it[2]])
+        sst = (ctypes.c_int * (5 * k))(*[x for it in items for x in it[3]])
+        dst = (ctypes.c_void_p * k)(*[it[4] for it in items])
+        dstr = (ctypes.c_int * k)(*[it[5] for it in items])
+        _check(lib().fft3d_batch_step(self.h, k, planes, ns, src, sst, dst, dstr,
+                                      ctypes.c_void_p(stream) if stream else None))
+
+    def stats(self) -> dict:
+        out = (ctypes.c_double * 8)()
+        _check(lib().fft3d_batch_stats(self.h, out))
+        return dict(steps=int(out[0]), graph_launches=int(out[1]), tuning_steps=int(out[2]),
+                    kernels_last_step=int(out[4]), step_shapes=int(out[5]))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fft3d_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -62,3 +62,15 @@ def test_defaults_match_reference():
     q = make_params()
     for name, _ in FFT3DParams._fields_:
         assert getattr(p, name) == pytest.approx(getattr(q, name)), name
+
+
+def test_batch_argument_checks_without_gpu():
+    L = engine.lib()
+    rc = L.fft3d_batch_step(None, 1, None, None, None, None, None, None, None)
+    assert rc == -1 and "invalid batch step" in L.fft3d_last_error().decode()
+    h = ctypes.c_void_p()
+    rc = L.fft3d_batch_create(0, ctypes.byref(h))
+    # no CUDA device in the CPU suite: refused before any work
+    assert rc in (0, -6)
+    if rc == 0:
+        L.fft3d_batch_destroy(h)
