@@ -153,12 +153,14 @@ int fft3d_filter2d_static(const fft3d_params* p, const fft3d_plane_desc* d, cons
  * one FFT3DEngine per plane per clip (src/fft3d.hpp:186-198, 241). One step
  * filters one output frame of each of `count` planes -- luma and chroma of
  * many clips, of mixed sizes, block sizes, bt and sample types -- with one
- * batched persistent launch per kernel variant and phase (forward,
- * filter/inverse, overlap-add) instead of three launches per plane. The
- * first steps of a new step shape are timed under candidate schedules
- * (persistent grid size, work-item order) and the fastest is kept per
- * launch (autotuner); the tuned step is captured into a CUDA graph and
- * replayed on later steps of that shape.
+ * batched persistent launch per kernel variant, phase (forward,
+ * filter/inverse, overlap-add) and wave instead of three launches per plane.
+ * A wave is a run of planes whose new spectra and time-domain blocks fit a
+ * byte budget, so that they can stay in L2 from one phase to the next. The
+ * first steps of a new step shape are timed under candidate wave budgets
+ * and then under candidate schedules per launch (persistent grid size,
+ * work-item order), keeping the fastest (autotuner); the tuned step is
+ * captured into a CUDA graph and replayed on later steps of that shape.
  * ------------------------------------------------------------------------ */
 typedef struct fft3d_batch fft3d_batch;
 
@@ -180,7 +182,8 @@ int fft3d_batch_step(fft3d_batch* b, int count, fft3d_plane* const* planes, cons
                      const int* src_stride, void* const* dst, const int* dst_stride, void* stream);
 
 /* out[0] steps, [1] graph launches, [2] tuning steps, [3] 0, [4] kernels
- * of the last step, [5] step shapes seen, [6..7] 0. */
+ * of the last step, [5] step shapes seen, [6] wave budget (MiB, 0 = one
+ * wave) of the last tuned step, [7] 0. */
 int fft3d_batch_stats(fft3d_batch* b, double out[8]);
 
 /* ------------------------------------------------------------------------

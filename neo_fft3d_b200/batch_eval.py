@@ -1,0 +1,184 @@
+"""Batched uneven-streams workload (needs a GPU).
+
+    python -m neo_fft3d_b200.batch_eval [--frames 60] [--seed 3000] [--mix uneven|small]
+
+mix "uneven" (default): 48 concurrent YUV420 streams of 60 frames: 16 at
+640x480 8-bit, 16 at 1280x720 8-bit, 12 at 1920x1080 8-bit and 4 at
+3840x2160 10-bit (uint16), per-stream seeds. mix "small": 48 streams at
+640x480 8-bit. Per stream: noise sigma uniform on [2, 10] (8-bit units, x4
+for 10-bit), bt uniform on {1..5}, bw = bh from {32, 48} with
+ow = oh = bw / 2; filter sigma = the noise sigma. Clips are generated on the
+device with the sinusoid-field formula of synth.make_clip.
+
+All planes are filtered per time step: (a) one plane at a time
+(fft3d_plane_filter_device, 3 launches per plane) on one stream, and (b) as
+one batched step (fft3d_batch_step: one persistent launch per kernel variant,
+phase and wave; autotuned; CUDA-graph replayed). Both passes are timed after
+a first untimed pass (which, for the batch, tunes and captures); the outputs
+of the two are compared byte for byte. Prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+
+import numpy as np
+
+from . import engine, synth
+from .params import make_params, plane_descs
+
+MIXES = {
+    "uneven": [(16, 640, 480, 8), (16, 1280, 720, 8), (12, 1920, 1080, 8), (4, 3840, 2160, 10)],
+    "small": [(48, 640, 480, 8)],
+}
+
+
+def streams(kinds, seed: int):
+    rng = np.random.default_rng(seed)
+    out = []
+    for count, w, h, bits in kinds:
+        for _ in range(count):
+            sigma = float(rng.uniform(2.0, 10.0))
+            bt = int(rng.integers(1, 6))
+            bw = int(rng.choice([32, 48]))
+            out.append(dict(width=w, height=h, bits=bits, sigma=sigma, bt=bt, bw=bw, seed=int(rng.integers(1 << 30))))
+    return out
+
+
+def make_clip_device(torch, width, height, frames, bits, noise_sigma, seed):
+    """synth.make_clip's field (64 sinusoids, sub-pixel motion, scaled to the
+    legal range) plus Gaussian noise, evaluated on the GPU; 3 planes (4:2:0)."""
+    shift = bits - 8
+    maxv = (1 << bits) - 1
+    rng_motion = np.random.default_rng([seed, 1])
+    steps = rng_motion.uniform(-2.0, 2.0, size=(frames, 2))
+    steps[0] = 0.0
+    path = np.cumsum(steps, axis=0)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    dtype = torch.uint8 if bits == 8 else torch.int16
+    planes = []
+    for p in range(3):
+        w = width >> 1 if p else width
+        h = height >> 1 if p else height
+        scale = 2.0 if p else 1.0
+        lo, hi = 16 << shift, (235 if p == 0 else 240) << shift
+        fx, fy, phase, amp = (torch.tensor(v, device="cuda", dtype=torch.float64)
+                              for v in synth._field_params(np.random.default_rng([seed, 10 + p])))
+
+        def field(dx, dy):
+            x = torch.arange(w, device="cuda", dtype=torch.float64) * scale - dx
+            y = torch.arange(h, device="cuda", dtype=torch.float64) * scale - dy
+            ax = 2 * math.pi * x[:, None] * fx[None, :]
+            by = 2 * math.pi * y[:, None] * fy[None, :] + phase[None, :]
+            return (torch.sin(by) * amp) @ torch.cos(ax).T + (torch.cos(by) * amp) @ torch.sin(ax).T
+
+        f0 = field(0.0, 0.0)
+        fmin, fmax = f0.min(), f0.max()
+        arr = torch.empty((frames, h, w), dtype=dtype, device="cuda")
+        for t in range(frames):
+            v = lo + (field(float(path[t][0]), float(path[t][1])) - fmin) * ((hi - lo) / (fmax - fmin))
+            v = v + torch.randn((h, w), generator=gen, device="cuda", dtype=torch.float64) * noise_sigma
+            arr[t] = torch.clamp(torch.round(v), 0, maxv).to(dtype)
+        planes.append(arr)
+    return planes
+
+
+def main():
+    import torch
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--frames", type=int, default=60)
+    ap.add_argument("--seed", type=int, default=3000)
+    ap.add_argument("--mix", default="uneven", choices=sorted(MIXES))
+    args = ap.parse_args()
+    F = args.frames
+    kinds = MIXES[args.mix]
+    cfg = streams(kinds, args.seed)
+    clips, engs, outs = [], [], []
+    canonical = 0.0
+    for s in cfg:
+        noise = s["sigma"] * (4 if s["bits"] == 10 else 1)
+        planes = make_clip_device(torch, s["width"], s["height"], F, s["bits"], noise, s["seed"])
+        p = make_params(sigma=s["sigma"], bt=s["bt"], bw=s["bw"], bh=s["bw"], ow=s["bw"] // 2, oh=s["bw"] // 2)
+        descs = plane_descs([tuple(a.shape[1:]) for a in planes], s["bits"], F)
+        for a, d in zip(planes, descs):
+            e = engine.PlaneEngine(p, d)
+            engs.append(e)
+            clips.append(a)
+            outs.append(torch.empty_like(a))
+            # canonical cached-spectrum bytes per output frame: pixels in,
+            # newest spectrum out, bt spectra in, pixels out
+            S = e.nblocks * s["bw"] * (s["bw"] // 2 + 1) * 8
+            P = a.shape[1] * a.shape[2] * a.element_size()
+            canonical += 2 * P + S + max(s["bt"], 1) * S
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+
+    def item(e, a, o, n):
+        fb = a.shape[1] * a.shape[2] * a.element_size()
+        ptrs = [a.data_ptr() + (n + k) * fb if 0 <= n + k < F else 0 for k in range(-2, 3)]
+        return e, n, ptrs, [a.shape[2] * a.element_size()] * 5, o.data_ptr() + n * fb, a.shape[2] * a.element_size()
+
+    def per_plane_pass():
+        for n in range(F):
+            for e, a, o in zip(engs, clips, outs):
+                _, _, ptrs, st, dst, ds = item(e, a, o, n)
+                e.filter_device(n, ptrs, st, dst, ds, stream.cuda_stream)
+
+    batch = engine.Batch(tuning=True)
+
+    def batched_pass():
+        for n in range(F):
+            batch.step([item(e, a, o, n) for e, a, o in zip(engs, clips, outs)], stream.cuda_stream)
+
+    def timed(fn):
+        for e in engs:
+            e.reset()
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        fn()
+        t1.record(stream)
+        torch.cuda.synchronize()
+        return t0.elapsed_time(t1) / 1000.0
+
+    timed(per_plane_pass)  # warm-up
+    l0 = engine.kernel_launches()
+    t_plane = timed(per_plane_pass)
+    launches_plane = engine.kernel_launches() - l0
+    ref = [o.clone() for o in outs]
+    timed(batched_pass)  # tunes and captures
+    l0 = engine.kernel_launches()
+    t_batch = timed(batched_pass)
+    launches_batch = engine.kernel_launches() - l0
+    same = all(bool(torch.equal(r, o)) for r, o in zip(ref, outs))
+    stats = batch.stats()
+    peak = None
+    peaks = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "MEASURED_PEAKS.json")
+    if os.path.exists(peaks):
+        with open(peaks) as f:
+            peak = float(json.load(f)["hbm_gbs"])
+    stream_frames = len(cfg) * F
+    line = dict(workload=f"batched_{len(cfg)}_{args.mix}_streams", frames_per_stream=F, streams=len(cfg),
+                planes=len(engs),
+                stream_frames_per_s=dict(per_plane=stream_frames / t_plane, batched=stream_frames / t_batch),
+                speedup=t_plane / t_batch,
+                kernels_per_step=dict(per_plane=launches_plane / F, batched=launches_batch / F),
+                canonical_bytes_per_step=canonical,
+                hbm_gbs=dict(per_plane=canonical * F / t_plane / 1e9, batched=canonical * F / t_batch / 1e9),
+                hbm_peak_gbs=peak, outputs_identical=same, batch_stats=stats,
+                mix={f"{w}x{h}/{b}bit": c for c, w, h, b in kinds},
+                bt_counts={str(k): sum(1 for s in cfg if s["bt"] == k) for k in range(1, 6)},
+                bw_counts={str(k): sum(1 for s in cfg if s["bw"] == k) for k in (32, 48)})
+    if peak:
+        line["hbm_frac"] = {k: v / peak for k, v in line["hbm_gbs"].items()}
+    print(json.dumps(line), flush=True)
+    batch.close()
+    for e in engs:
+        e.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -6,16 +6,24 @@
 // ring, btcur edges, Kalman passthrough, crop) while the launches are
 // recorded instead of issued (fft3d::plane_plan). The records are grouped by
 // kernel variant -- forward by (bw, bh, sample type), filter/inverse by
-// (bw, bh, mode), plane copies, overlap-add by sample type -- and each group becomes ONE
-// launch whose CTAs walk a list of (plane, CTA-of-that-plane) work items, so
-// a step of 48 clips x 3 planes is ~3-12 launches instead of ~430.
+// (bw, bh, mode), plane copies, overlap-add by sample type -- and each group
+// becomes ONE launch whose CTAs walk a list of (plane, CTA-of-that-plane)
+// work items, so a step of 48 clips x 3 planes is tens of launches instead of
+// ~430.
 //
-// Autotuner. The step's shape (groups and their per-plane work items) is
-// its signature. The first steps of a new signature try each candidate
-// schedule -- persistent grid of 1, 2, 4 or all resident CTAs per SM, or one
-// CTA per work item; work items plane-major or interleaved across planes --
-// timing every group's launch with CUDA events, and keep the fastest
-// schedule per group. The tuned step is then captured once into a CUDA graph
+// Waves. Launching each phase over ALL planes streams the new spectra and
+// time-domain blocks of every plane through HBM between the phases, while a
+// plane filtered on its own finds them in L2. So a step can be cut into waves
+// of consecutive planes whose new spectra + time-domain blocks fit a byte
+// budget, the phases running wave by wave.
+//
+// Autotuner. The step's shape (variants and per-plane work items) is its
+// signature. The first steps of a new signature time the whole step under
+// each candidate wave budget (24..192 MiB, or one wave), then time every
+// launch under each candidate schedule -- persistent grid of 1, 2, 4 or all
+// resident CTAs per SM, or one CTA per work item; work items plane-major or
+// interleaved across planes -- and keep the fastest budget and the fastest
+// schedule per launch. The tuned step is then captured once into a CUDA graph
 // (argument upload from pinned staging + the launches); later steps of that
 // signature only rewrite the pinned arguments and launch the graph. Two
 // graph instances alternate over two staging buffers so that the host can
@@ -63,8 +71,15 @@ constexpr int kNumCand = sizeof(kCandidates) / sizeof(kCandidates[0]);
 // before the overlap-add, which writes the interior over them
 enum Phase { PH_FWD = 0, PH_INV = 1, PH_COPY = 2, PH_OLA = 3 };
 
+// Wave budgets tried by the tuner: the new spectra and time-domain blocks of
+// the planes of one wave (forward -> filter/inverse -> overlap-add) should
+// stay in the 126 MB L2 between the phases; 0 = all planes in one wave.
+const size_t kBudgets[] = {size_t(24) << 20, size_t(48) << 20, size_t(96) << 20, size_t(192) << 20, 0};
+constexpr int kNumBudgets = sizeof(kBudgets) / sizeof(kBudgets[0]);
+constexpr size_t kDefaultBudget = 0;
+
 struct Group {
-  int phase, bw, bh, var;   // var: bytes per sample (forward, overlap-add) or filter mode
+  int wave, phase, bw, bh, var;  // var: bytes per sample (forward, overlap-add) or filter mode
   std::vector<int> recs;    // indices into the Deferred vector of the phase
   std::vector<int> per;     // work items per record
   int nitems = 0;
@@ -81,9 +96,11 @@ struct Plan {
 };
 
 struct Tune {
-  int next = 0;                             // next candidate to try
-  std::vector<std::vector<float>> ms;      // [group][candidate]
-  bool done = false;
+  int stage = 0;                       // 0: wave budget, 1: per-launch schedule, 2: done
+  int next = 0;                        // next candidate of the stage
+  std::vector<float> budget_ms;        // whole-step time per budget
+  size_t budget = kDefaultBudget;
+  std::vector<std::vector<float>> ms;  // [group][schedule candidate]
   std::vector<Sched> best;
 };
 
@@ -143,21 +160,50 @@ struct fft3d_batch {
   void* h_direct = nullptr;
   size_t h_direct_cap = 0;
   cudaEvent_t direct_done = nullptr;
-  double stats[8] = {};  // steps, graph launches, tuning steps, -, kernels of the last step, step shapes
+  double stats[8] = {};  // steps, graph launches, tuning steps, -, kernels of the last step, step shapes,
+                         // wave budget (MiB) of the last tuned step
 };
 
 namespace {
 
-void build_groups(const Deferred& d, Plan& plan) {
-  std::map<std::tuple<int, int, int, int>, int> index;
+int rec_plane(const Deferred& d, int phase, int r) {
+  switch (phase) {
+    case PH_FWD: return d.fwd[r].plane;
+    case PH_INV: return d.inv[r].plane;
+    case PH_COPY: return d.copies[r].plane;
+    default: return d.ola[r].plane;
+  }
+}
+
+// Groups the records by (wave, phase, kernel variant); budget 0 = one wave.
+void build_groups(const Deferred& d, int nplanes, size_t budget, Plan& plan) {
+  std::vector<double> weight(nplanes, 0.0);
+  for (const auto& r : d.inv) {
+    const fft3d::Geom& g = r.a.g;
+    weight[r.plane] += (double)g.nblocks * g.bh * (g.bw / 2 + 1) * 8 + (double)g.nblocks * g.bh * g.bw * 4;
+  }
+  std::vector<int> wave(nplanes, 0);
+  int w = 0;
+  double acc = 0.0;
+  for (int p = 0; p < nplanes; p++) {
+    if (budget && acc > 0.0 && acc + weight[p] > (double)budget) {
+      w++;
+      acc = 0.0;
+    }
+    wave[p] = w;
+    acc += weight[p];
+  }
+  std::map<std::tuple<int, int, int, int, int>, int> index;
   auto add = [&](int phase, int r, int bw, int bh, int var) {
-    auto key = std::make_tuple(phase, bw, bh, var);
+    const int wv = wave[rec_plane(d, phase, r)];
+    auto key = std::make_tuple(wv, phase, bw, bh, var);
     auto it = index.find(key);
     int gi;
     if (it == index.end()) {
       gi = (int)plan.groups.size();
       index[key] = gi;
       Group g;
+      g.wave = wv;
       g.phase = phase;
       g.bw = bw;
       g.bh = bh;
@@ -179,8 +225,9 @@ void build_groups(const Deferred& d, Plan& plan) {
   for (int r = 0; r < (int)d.inv.size(); r++) add(PH_INV, r, d.inv[r].a.g.bw, d.inv[r].a.g.bh, d.inv[r].mode);
   for (int r = 0; r < (int)d.copies.size(); r++) add(PH_COPY, r, 0, 0, 0);
   for (int r = 0; r < (int)d.ola.size(); r++) add(PH_OLA, r, 0, 0, d.ola[r].bytes);
-  // phases in order; within a phase the larger groups first
+  // waves in order, phases in order within a wave; the larger groups first
   std::stable_sort(plan.groups.begin(), plan.groups.end(), [](const Group& a, const Group& b) {
+    if (a.wave != b.wave) return a.wave < b.wave;
     return a.phase != b.phase ? a.phase < b.phase : a.nitems > b.nitems;
   });
   std::string sig;
@@ -189,8 +236,8 @@ void build_groups(const Deferred& d, Plan& plan) {
     g.arg_size = arg_size(g.phase);
     g.args_off = off;
     off = align_up(off + g.arg_size * g.recs.size(), 256);
-    sig += std::to_string(g.phase) + "/" + std::to_string(g.bw) + "x" + std::to_string(g.bh) + "/" +
-           std::to_string(g.var) + ":";
+    sig += std::to_string(g.wave) + "/" + std::to_string(g.phase) + "/" + std::to_string(g.bw) + "x" +
+           std::to_string(g.bh) + "/" + std::to_string(g.var) + ":";
     for (int n : g.per) sig += std::to_string(n) + ",";
     sig += ";";
   }
@@ -391,26 +438,55 @@ int fft3d_batch_step(fft3d_batch* b, int count, fft3d_plane* const* planes, cons
   for (auto* P : order) locks.emplace_back(fft3d::plane_mutex(P));
   Deferred d;
   for (int i = 0; i < count; i++) {
+    d.plane = i;
     int rc = fft3d::plane_plan(planes[i], n[i], src + 5 * i, src_stride + 5 * i, dst[i], dst_stride[i], s, &d);
     if (rc) return rc;
   }
   cudaSetDevice(b->device);
-  Plan plan;
-  build_groups(d, plan);
+  Plan shape;  // the step's shape (one wave) keys its tuning
+  build_groups(d, count, 0, shape);
+  Tune& t = b->tunes[shape.sig];
   b->stats[0] += 1;
+  if (t.budget_ms.empty()) {
+    t.budget_ms.assign(kNumBudgets, 0.f);
+    b->stats[5] += 1;
+    if (!b->tuning) t.stage = 2;
+  }
+  Plan plan;
+  if (t.stage == 0) {
+    // tuning, stage 0: the wave budget, default schedules, whole step timed
+    build_groups(d, count, kBudgets[t.next], plan);
+    set_grids(b, plan);
+    cudaEvent_t ev[2];
+    cudaEventCreate(&ev[0]);
+    cudaEventCreate(&ev[1]);
+    cudaEventRecord(ev[0], s);
+    int rc = run_direct(b, plan, d, s, nullptr);
+    cudaEventRecord(ev[1], s);
+    if (rc == FFT3D_OK) {
+      cudaError_t e = cudaEventSynchronize(ev[1]);
+      if (e != cudaSuccess) rc = cuda_fail(e, "batch tuning");
+      else cudaEventElapsedTime(&t.budget_ms[t.next], ev[0], ev[1]);
+    }
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    if (rc) return rc;
+    b->stats[2] += 1;
+    b->stats[4] = (double)plan.groups.size();
+    fft3d::count_launches(plan.groups.size());
+    if (++t.next == kNumBudgets) {
+      t.budget = kBudgets[std::min_element(t.budget_ms.begin(), t.budget_ms.end()) - t.budget_ms.begin()];
+      t.stage = 1;
+      t.next = 0;
+    }
+    return FFT3D_OK;
+  }
+  build_groups(d, count, t.budget, plan);
   b->stats[4] = (double)plan.groups.size();
   fft3d::count_launches(plan.groups.size());
-  Tune& t = b->tunes[plan.sig];
-  if (t.ms.empty()) {
-    t.ms.assign(plan.groups.size(), std::vector<float>(kNumCand, 0.f));
-    b->stats[5] += 1;
-    if (!b->tuning) {
-      t.done = true;
-      t.best.assign(plan.groups.size(), Sched{64, 0});
-    }
-  }
-  if (!t.done) {
-    // tuning step: candidate t.next for every group, each launch timed
+  if (t.stage == 1) {
+    // tuning, stage 1: one schedule candidate for every launch, each launch timed
+    if (t.ms.empty()) t.ms.assign(plan.groups.size(), std::vector<float>(kNumCand, 0.f));
     for (auto& g : plan.groups) g.sched = kCandidates[t.next];
     set_grids(b, plan);
     std::vector<cudaEvent_t> ev(2 * plan.groups.size());
@@ -421,7 +497,8 @@ int fft3d_batch_step(fft3d_batch* b, int count, fft3d_plane* const* planes, cons
       if (e != cudaSuccess) rc = cuda_fail(e, "batch tuning");
     }
     if (rc == FFT3D_OK)
-      for (size_t gi = 0; gi < plan.groups.size(); gi++) cudaEventElapsedTime(&t.ms[gi][t.next], ev[2 * gi], ev[2 * gi + 1]);
+      for (size_t gi = 0; gi < plan.groups.size(); gi++)
+        cudaEventElapsedTime(&t.ms[gi][t.next], ev[2 * gi], ev[2 * gi + 1]);
     for (auto& e : ev) cudaEventDestroy(e);
     if (rc) return rc;
     b->stats[2] += 1;
@@ -431,12 +508,14 @@ int fft3d_batch_step(fft3d_batch* b, int count, fft3d_plane* const* planes, cons
         const auto& m = t.ms[gi];
         t.best[gi] = kCandidates[std::min_element(m.begin(), m.end()) - m.begin()];
       }
-      t.done = true;
+      t.stage = 2;
     }
     return FFT3D_OK;
   }
-  for (size_t gi = 0; gi < plan.groups.size(); gi++) plan.groups[gi].sched = t.best[gi];
+  if (t.best.size() == plan.groups.size())
+    for (size_t gi = 0; gi < plan.groups.size(); gi++) plan.groups[gi].sched = t.best[gi];
   set_grids(b, plan);
+  b->stats[6] = (double)(t.budget >> 20);
   auto& slot = b->graphs[plan.sig];
   if (!slot) {
     slot.reset(new Captured);

@@ -15,10 +15,11 @@ namespace fft3d {
 // Launches and device copies of one output frame of one plane, recorded in
 // issue order by phase instead of being issued.
 struct Deferred {
-  struct Fwd { ForwardArgs a; int bytes; };
-  struct Inv { InverseArgs a; int mode; };
-  struct Ola { OlaArgs a; int bytes; };
-  struct Copy { void* dst; size_t dpitch; const void* src; size_t spitch; size_t width; size_t height; };
+  struct Fwd { ForwardArgs a; int bytes; int plane; };
+  struct Inv { InverseArgs a; int mode; int plane; };
+  struct Ola { OlaArgs a; int bytes; int plane; };
+  struct Copy { void* dst; size_t dpitch; const void* src; size_t spitch; size_t width; size_t height; int plane; };
+  int plane = 0;  // index of the plane being planned (tags the records)
   std::vector<Fwd> fwd;
   std::vector<Inv> inv;
   std::vector<Ola> ola;

@@ -312,7 +312,7 @@ fft3d::ForwardArgs forward_args(fft3d_plane* P, const void* plane, long long str
 int launch_forward(fft3d_plane* P, const void* plane, long long stride, float2* spec, cudaStream_t st) {
   fft3d::ForwardArgs a = forward_args(P, plane, stride, spec);
   if (g_defer) {
-    g_defer->fwd.push_back({a, P->bytes});
+    g_defer->fwd.push_back({a, P->bytes, g_defer->plane});
     return FFT3D_OK;
   }
   TimeScope ts(P, K_FORWARD, (double)P->g.W * P->g.H * P->bytes + (double)P->spec_elems() * sizeof(float2), st);
@@ -355,7 +355,7 @@ int copy_plane(fft3d_plane* P, void* dst, int dstride, const void* src, int sstr
                cudaStream_t st) {
   if (g_defer && kind == cudaMemcpyDeviceToDevice) {
     g_defer->copies.push_back({dst, (size_t)dstride, src, (size_t)sstride, (size_t)P->d.width * P->bytes,
-                               (size_t)P->d.height});
+                               (size_t)P->d.height, g_defer->plane});
     return FFT3D_OK;
   }
   CK(cudaMemcpy2DAsync(dst, dstride, src, sstride, (size_t)P->d.width * P->bytes, P->d.height, kind, st),
@@ -484,7 +484,7 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
       TimeScope ts(P, K_INVERSE, S + T, st);
       CK(fft3d::launch_filter_inverse(sa, fft3d::MODE_SHARPEN_ONLY, st), "sharpen/inverse kernel");
     } else if (g_defer) {
-      g_defer->inv.push_back({ia, mode});
+      g_defer->inv.push_back({ia, mode, g_defer->plane});
     } else {
       // reads: the spectra of the window (+ Kalman state); writes: the time-domain blocks
       TimeScope ts(P, K_INVERSE, (to - from + 1) * S + state + T, st);
@@ -526,7 +526,7 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
   oa.base = (ints && P->d.is_chroma) ? (float)(1 << (P->d.bits - 1)) : 0.f;
   oa.maxval = P->bytes == 1 ? 255 : (1 << P->d.bits) - 1;
   if (g_defer) {
-    g_defer->ola.push_back({oa, P->bytes});
+    g_defer->ola.push_back({oa, P->bytes, g_defer->plane});
   } else {
     TimeScope ts(P, K_OLA, (double)P->g.nblocks * P->g.bh * P->g.bw * 4 + (double)P->g.W * P->g.H * P->bytes, st);
     CK(fft3d::launch_overlap_add(oa, P->bytes, st), "overlap-add kernel");

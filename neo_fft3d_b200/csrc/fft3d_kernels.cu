@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(kOlaTx * kOlaTy) k_overlap_add_batch(const Ola
                                                                       const int2* __restrict__ items, int nitems) {
   for (int i = blockIdx.x; i < nitems; i += gridDim.x) {
     const int2 it = items[i];
-    const OlaArgs& a = args[it.x];
+    const OlaArgs a = args[it.x];  // private copy: fields stay in registers
     const int tx = (a.g.W + kOlaTx - 1) / kOlaTx;
     const int ty = it.y / tx, t = it.y - ty * tx;
     overlap_add_px<T>(a, t * kOlaTx + threadIdx.x, ty * kOlaTy + threadIdx.y);
@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(256) k_copy_batch(const CopyArgs* __restrict__
                                                     int nitems) {
   for (int i = blockIdx.x; i < nitems; i += gridDim.x) {
     const int2 it = items[i];
-    const CopyArgs& c = args[it.x];
+    const CopyArgs c = args[it.x];
     const char* s = static_cast<const char*>(c.src) + (long long)it.y * c.spitch;
     char* d = static_cast<char*>(c.dst) + (long long)it.y * c.dpitch;
     if ((((uintptr_t)s | (uintptr_t)d) & 15) == 0) {

@@ -245,7 +245,9 @@ __global__ void __launch_bounds__(kWarps * 32) k_forward_batch(const ForwardArgs
                                                               const int2* __restrict__ items, int nitems) {
   for (int i = blockIdx.x; i < nitems; i += gridDim.x) {
     const int2 it = items[i];
-    forward_cta<BW, BH, T>(args[it.x], it.y);
+    // a private copy: the body's stores cannot alias it, so its fields stay in registers
+    const ForwardArgs a = args[it.x];
+    forward_cta<BW, BH, T>(a, it.y);
   }
 }
 
@@ -560,12 +562,22 @@ __global__ void __launch_bounds__(kWarps * 32) k_filter_inverse(InverseArgs a) {
   filter_inverse_cta<BW, BH, MODE>(a, blockIdx.x);
 }
 
+// The work item's arguments are staged in shared memory: the body's global
+// stores cannot alias them (a reference into global memory would be reloaded
+// after every store), and unlike a by-value copy they cost no registers.
 template <int BW, int BH, int MODE>
 __global__ void __launch_bounds__(kWarps * 32) k_filter_inverse_batch(const InverseArgs* __restrict__ args,
                                                                      const int2* __restrict__ items, int nitems) {
+  __shared__ __align__(16) InverseArgs sa;
+  static_assert(sizeof(InverseArgs) % 4 == 0, "word copy");
   for (int i = blockIdx.x; i < nitems; i += gridDim.x) {
     const int2 it = items[i];
-    filter_inverse_cta<BW, BH, MODE>(args[it.x], it.y);
+    __syncthreads();  // every warp is done with the previous item's arguments
+    const int* src = reinterpret_cast<const int*>(args + it.x);
+    int* dst = reinterpret_cast<int*>(&sa);
+    for (int w = threadIdx.x; w < (int)(sizeof(InverseArgs) / 4); w += blockDim.x) dst[w] = src[w];
+    __syncthreads();
+    filter_inverse_cta<BW, BH, MODE>(sa, it.y);
   }
 }
 
