@@ -11,12 +11,19 @@ output frame, edge frames with bt=1 as the reference does), inputs resident
 in HBM. The clip (373 MB) and the spectrum ring (~350 MB) are larger than L2,
 so no flush is needed between steps.
 
+Both forms of the block transform run K timed steps each: the plain FP32
+register FFT and the tensor-core split-precision BF16 DFT-GEMM (32x32
+blocks); their outputs are compared pixel by pixel (within +-1 LSB).
+
 Lines printed (rank 0, one JSON line):
-  value      frames/s of the device-resident path (whole job over N ranks)
+  value      frames/s of the faster form, device-resident (whole job over N ranks)
+  paths      frames/s of both forms, their ratio and output agreement
   e2e        frames/s through the C ABI with host buffers (pinned), copies in
   roofline   the dominant kernel's algorithmic bytes / its CUDA-event time
   cpu_baseline  the reference plugin (built from its sources, oracle/_ref) on
              a bounded sample of the same workload on this host's cores
+  kalman_4k10_bw48  the Kalman workload (60 frames 4K 10-bit YUV420, scene cut
+             at frame 30, bt=0, bw=bh=48, ow=oh=16): frames/s and its frame roofline
 ``--impl reference`` times only the reference's CPU implementation.
 Multi-GPU (torchrun): independent replicas, one clip per rank, no collective
 on the data path ("scaling": "weak").
@@ -40,8 +47,10 @@ import numpy as np  # noqa: E402
 from neo_fft3d_b200 import synth  # noqa: E402
 
 WORKLOAD = "1080p_bt5_bw32"
-METRIC = "1080p bt=5 frames/s (120-frame YUV420 8-bit clip, bw=bh=32, ow=oh=16, sharpen=0.3)"
+METRIC = "1080p bt=5 frames/s: TC split-precision vs plain FP32 kernel at \u00b11 LSB; %HBM roofline"
 UNIT = "frames/s"
+# the two forms of the block transform that the metric compares (NEO_FFT3D_PATH)
+PATHS = {"plain_fp32": "unfused", "tc_split_bf16": "tc"}
 
 
 def workload():
@@ -163,6 +172,64 @@ def reference_arm(args, rank):
     return line
 
 
+def kalman_4k(args, torch, dist, engine, make_params, plane_descs, local, world, steps=3):
+    """The Kalman workload: 60 frames of 3840x2160 10-bit YUV420 (noise sigma 12
+    in 10-bit codes, scene cut at frame 30), bt=0, sigma=3, kratio=2,
+    bw=bh=48, ow=oh=16; one step = the whole clip from frame 0 (state reset),
+    planes on their own streams. Frame roofline: the minimal-state byte model
+    2 P + 32 B per bin (pixels in and out; the spectrum's re/im and the
+    Kalman state's last value and two covariances, read and written)."""
+    F = 60
+    planes = synth.make_clip_device(3840, 2160, F, bits=10, noise_sigma=12.0, seed=1002, scene_cut=30)
+    p = make_params(sigma=3.0, bt=0, kratio=2.0, bw=48, bh=48, ow=16, oh=16)
+    descs = plane_descs([tuple(a.shape[1:]) for a in planes], 10, F)
+    engs = [engine.PlaneEngine(p, d, local) for d in descs]
+    outs = [torch.empty_like(a) for a in planes]
+    streams = [torch.cuda.Stream() for _ in engs]
+    master = torch.cuda.current_stream()
+
+    def step():
+        ev = torch.cuda.Event()
+        ev.record(master)
+        for e, a, o, s in zip(engs, planes, outs, streams):
+            s.wait_event(ev)
+            e.reset()
+            fb = a.shape[1] * a.shape[2] * 2
+            for n in range(F):
+                ptrs = [0, 0, a.data_ptr() + n * fb, 0, 0]
+                e.filter_device(n, ptrs, [a.shape[2] * 2] * 5, o.data_ptr() + n * fb, a.shape[2] * 2, s.cuda_stream)
+        for s in streams:
+            master.wait_stream(s)
+
+    step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(master)
+    for _ in range(steps):
+        step()
+    t1.record(master)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    if world > 1:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    fps = world * F * steps / (ms / 1000.0)
+    P = sum(a[0].numel() * 2 for a in planes)
+    bins = sum(e.nblocks * 48 * 25 for e in engs)
+    fb = 2 * P + 32 * bins
+    peak, kind = load_peaks()
+    for e in engs:
+        e.close()
+    return {"value": fps, "unit": UNIT, "frames_per_step": F, "steps": steps, "ms_per_step": ms / steps,
+            "config": {"width": 3840, "height": 2160, "format": "YUV420P10", "bt": 0, "sigma": 3.0, "kratio": 2.0,
+                       "bw": 48, "bh": 48, "ow": 16, "oh": 16, "scene_cut": 30, "noise_sigma": 12},
+            "frame_roofline": {"bytes_per_frame": fb, "achieved_gbs": fb * fps / world / 1e9,
+                               "frac": fb * fps / world / 1e9 / peak, "peak_kind": kind}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -171,6 +238,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-kalman", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -202,53 +270,82 @@ def main():
     p = make_params(**filt)
     descs = plane_descs([a.shape[1:] for a in planes], 8, F)
     dev = [torch.from_numpy(a).cuda() for a in planes]
-    outs = [torch.empty_like(d) for d in dev]
-    engs = [engine.PlaneEngine(p, d, local) for d in descs]
-    streams = [torch.cuda.Stream() for _ in engs]
     master = torch.cuda.current_stream()
 
-    def step(serial=False):
-        ev = torch.cuda.Event()
-        ev.record(master)
-        for i, e in enumerate(engs):
-            s = master if serial else streams[i]
-            s.wait_event(ev)
-            a, o = dev[i], outs[i]
-            W = a.shape[2]
-            fb = a.shape[1] * W
-            base = a.data_ptr()
-            obase = o.data_ptr()
-            for n in range(F):
-                ptrs = [base + (n + d) * fb if 0 <= n + d < F else 0 for d in range(-2, 3)]
-                e.filter_device(n, ptrs, [W] * 5, obase + n * fb, W, s.cuda_stream)
-        for s in streams:
-            master.wait_stream(s)
+    def make_arm(path):
+        os.environ["NEO_FFT3D_PATH"] = path
+        engs = [engine.PlaneEngine(p, d, local) for d in descs]
+        outs = [torch.empty_like(d) for d in dev]
+        streams = [torch.cuda.Stream() for _ in engs]
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+        def step(serial=False):
+            ev = torch.cuda.Event()
+            ev.record(master)
+            for i, e in enumerate(engs):
+                s = master if serial else streams[i]
+                s.wait_event(ev)
+                a, o = dev[i], outs[i]
+                W = a.shape[2]
+                fb = a.shape[1] * W
+                base = a.data_ptr()
+                obase = o.data_ptr()
+                for n in range(F):
+                    ptrs = [base + (n + d) * fb if 0 <= n + d < F else 0 for d in range(-2, 3)]
+                    e.filter_device(n, ptrs, [W] * 5, obase + n * fb, W, s.cuda_stream)
+            for s in streams:
+                master.wait_stream(s)
+
+        return {"engs": engs, "outs": outs, "step": step}
+
+    def time_arm(arm):
+        for _ in range(args.warmup):
+            arm["step"]()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        l0 = engine.kernel_launches()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        t0.record(master)
+        for _ in range(args.steps):
+            arm["step"]()
+        t1.record(master)
+        torch.cuda.synchronize()
+        arm["launches"] = engine.kernel_launches() - l0
+        ms = t0.elapsed_time(t1)
+        if world > 1:
+            tt = torch.tensor([ms], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = float(tt.item())
+            dist.barrier()
+        arm["ms"] = ms
+        arm["value"] = world * F * args.steps / (ms / 1000.0)
+
+    arms = {name: make_arm(path) for name, path in PATHS.items()}
+    os.environ["NEO_FFT3D_PATH"] = PATHS["plain_fp32"]
     clocks = ClockSampler(local)
     clocks.start()
-    l0 = engine.kernel_launches()
-    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    t0.record(master)
-    for _ in range(args.steps):
-        step()
-    t1.record(master)
-    torch.cuda.synchronize()
-    launches = engine.kernel_launches() - l0
+    for arm in arms.values():
+        time_arm(arm)
     clk = clocks.stop()
-    ms = t0.elapsed_time(t1)
-    if world > 1:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
-        dist.barrier()
-    ms_per_step = ms / args.steps
-    value = world * F * args.steps / (ms / 1000.0)
+    head_name = max(arms, key=lambda k: arms[k]["value"])
+    head = arms[head_name]
+    engs = head["engs"]
+    step = head["step"]
+    value = head["value"]
+    ms_per_step = head["ms"] / args.steps
+    launches = head["launches"]
+    # the two forms' outputs (the last step wrote every frame of every plane)
+    diff_max, within, total_px = 0, 0, 0
+    for a, b in zip(arms["plain_fp32"]["outs"], arms["tc_split_bf16"]["outs"]):
+        d = (a.to(torch.int16) - b.to(torch.int16)).abs()
+        diff_max = max(diff_max, int(d.max().item()))
+        within += int((d <= 1).sum().item())
+        total_px += d.numel()
+    paths = {name: {"value": arm["value"], "ms_per_step": arm["ms"] / args.steps, "launches": arm["launches"],
+                    "NEO_FFT3D_PATH": PATHS[name]} for name, arm in arms.items()}
+    paths["tc_over_plain"] = arms["tc_split_bf16"]["value"] / arms["plain_fp32"]["value"]
+    paths["tc_vs_plain_output"] = {"within_1lsb": within / total_px, "max_abs_diff": diff_max, "pixels": total_px}
 
     # per-kernel roofline from an instrumented pass (events around each
     # launch; planes serialised on one stream so that no other kernel shares
@@ -319,6 +416,8 @@ def main():
                "h2d_bytes_per_step": F * frame_bytes, "d2h_bytes_per_step": F * frame_bytes,
                "path": "fft3d_plane_filter (host API), one host thread per plane, pinned buffers"}
 
+    kalman = None if args.no_kalman else kalman_4k(args, torch, dist, engine, make_params, plane_descs, local, world)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -340,15 +439,16 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "frames_per_step": F, "width": 1920, "height": 1080,
                        "format": "YUV420P8", "bt": 5, "sigma": 3.0, "bw": 32, "bh": 32, "ow": 16, "oh": 16,
-                       "sharpen": 0.3, "path": "plain_fp32/" + os.environ.get("NEO_FFT3D_PATH", "unfused"),
+                       "sharpen": 0.3, "path": head_name,
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (373 MB clip + ~350 MB spectrum ring per rank), no flush"},
             "roofline": roofline, "frame_roofline": frame_roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "clocks": clk, "gpu_launches": launches,
+            "clocks": clk, "gpu_launches": launches, "paths": paths, "kalman_4k10_bw48": kalman,
         }
         print(json.dumps(line), flush=True)
-    for e in engs:
-        e.close()
+    for arm in arms.values():
+        for e in arm["engs"]:
+            e.close()
     if world > 1:
         dist.destroy_process_group()
 

@@ -21,7 +21,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 
 import numpy as np
@@ -47,45 +46,6 @@ def streams(kinds, seed: int):
     return out
 
 
-def make_clip_device(torch, width, height, frames, bits, noise_sigma, seed):
-    """synth.make_clip's field (64 sinusoids, sub-pixel motion, scaled to the
-    legal range) plus Gaussian noise, evaluated on the GPU; 3 planes (4:2:0)."""
-    shift = bits - 8
-    maxv = (1 << bits) - 1
-    rng_motion = np.random.default_rng([seed, 1])
-    steps = rng_motion.uniform(-2.0, 2.0, size=(frames, 2))
-    steps[0] = 0.0
-    path = np.cumsum(steps, axis=0)
-    gen = torch.Generator(device="cuda")
-    gen.manual_seed(seed)
-    dtype = torch.uint8 if bits == 8 else torch.int16
-    planes = []
-    for p in range(3):
-        w = width >> 1 if p else width
-        h = height >> 1 if p else height
-        scale = 2.0 if p else 1.0
-        lo, hi = 16 << shift, (235 if p == 0 else 240) << shift
-        fx, fy, phase, amp = (torch.tensor(v, device="cuda", dtype=torch.float64)
-                              for v in synth._field_params(np.random.default_rng([seed, 10 + p])))
-
-        def field(dx, dy):
-            x = torch.arange(w, device="cuda", dtype=torch.float64) * scale - dx
-            y = torch.arange(h, device="cuda", dtype=torch.float64) * scale - dy
-            ax = 2 * math.pi * x[:, None] * fx[None, :]
-            by = 2 * math.pi * y[:, None] * fy[None, :] + phase[None, :]
-            return (torch.sin(by) * amp) @ torch.cos(ax).T + (torch.cos(by) * amp) @ torch.sin(ax).T
-
-        f0 = field(0.0, 0.0)
-        fmin, fmax = f0.min(), f0.max()
-        arr = torch.empty((frames, h, w), dtype=dtype, device="cuda")
-        for t in range(frames):
-            v = lo + (field(float(path[t][0]), float(path[t][1])) - fmin) * ((hi - lo) / (fmax - fmin))
-            v = v + torch.randn((h, w), generator=gen, device="cuda", dtype=torch.float64) * noise_sigma
-            arr[t] = torch.clamp(torch.round(v), 0, maxv).to(dtype)
-        planes.append(arr)
-    return planes
-
-
 def main():
     import torch
     ap = argparse.ArgumentParser()
@@ -100,7 +60,7 @@ def main():
     canonical = 0.0
     for s in cfg:
         noise = s["sigma"] * (4 if s["bits"] == 10 else 1)
-        planes = make_clip_device(torch, s["width"], s["height"], F, s["bits"], noise, s["seed"])
+        planes = synth.make_clip_device(s["width"], s["height"], F, bits=s["bits"], noise_sigma=noise, seed=s["seed"])
         p = make_params(sigma=s["sigma"], bt=s["bt"], bw=s["bw"], bh=s["bw"], ow=s["bw"] // 2, oh=s["bw"] // 2)
         descs = plane_descs([tuple(a.shape[1:]) for a in planes], s["bits"], F)
         for a, d in zip(planes, descs):

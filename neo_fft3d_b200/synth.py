@@ -87,6 +87,60 @@ def make_clip(width: int, height: int, frames: int, *, bits: int = 8, noise_sigm
     return (out, clean_out) if with_clean else out
 
 
+def make_clip_device(width: int, height: int, frames: int, *, bits: int = 8, noise_sigma: float = 4.0, seed: int = 0,
+                     ssw: int = 1, ssh: int = 1, scene_cut: int | None = None, planes: int = 3):
+    """make_clip's clip evaluated on the GPU (torch, FP64 field, device RNG for
+    the noise): the same field, motion and scaling, for workloads too large to
+    generate on the host quickly. Returns a list of CUDA tensors [F, H, W],
+    uint8 for 8-bit and int16 (same bit patterns as uint16) for 9..15-bit."""
+    import math
+
+    import torch
+    shift = bits - 8
+    maxv = (1 << bits) - 1
+    rng_motion = np.random.default_rng([seed, 1])
+    steps = rng_motion.uniform(-2.0, 2.0, size=(frames, 2))
+    steps[0] = 0.0
+    path = np.cumsum(steps, axis=0)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    dtype = torch.uint8 if bits <= 8 else torch.int16
+    out = []
+    for p in range(planes):
+        w = width >> ssw if p else width
+        h = height >> ssh if p else height
+        scale = float(1 << ssw) if p else 1.0
+        lo, hi = 16 << shift, (235 if p == 0 else 240) << shift
+
+        def params(s):
+            return [torch.tensor(v, device="cuda", dtype=torch.float64)
+                    for v in _field_params(np.random.default_rng([s, 10 + p]))]
+
+        def field(prm, dx, dy):
+            fx, fy, phase, amp = prm
+            x = torch.arange(w, device="cuda", dtype=torch.float64) * scale - dx
+            y = torch.arange(h, device="cuda", dtype=torch.float64) * scale - dy
+            ax = 2 * math.pi * x[:, None] * fx[None, :]
+            by = 2 * math.pi * y[:, None] * fy[None, :] + phase[None, :]
+            return (torch.sin(by) * amp) @ torch.cos(ax).T + (torch.cos(by) * amp) @ torch.sin(ax).T
+
+        prm = params(seed)
+        f0 = field(prm, 0.0, 0.0)
+        fmin, fmax = f0.min(), f0.max()
+        arr = torch.empty((frames, h, w), dtype=dtype, device="cuda")
+        for t in range(frames):
+            if scene_cut is not None and t == scene_cut:
+                prm = params(seed + 7919)
+                f0 = field(prm, 0.0, 0.0)
+                fmin, fmax = f0.min(), f0.max()
+            v = lo + (field(prm, float(path[t][0]), float(path[t][1])) - fmin) * ((hi - lo) / (fmax - fmin))
+            if noise_sigma > 0:
+                v = v + torch.randn((h, w), generator=gen, device="cuda", dtype=torch.float64) * noise_sigma
+            arr[t] = torch.clamp(torch.round(v), 0, maxv).to(dtype)
+        out.append(arr)
+    return out
+
+
 def pack(planes) -> np.ndarray:
     """Pack a clip (list of [F,H,W] planes) into one contiguous byte buffer:
     frame after frame, planes in order, rows without padding."""
