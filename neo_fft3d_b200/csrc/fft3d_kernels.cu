@@ -8,7 +8,23 @@
 #include "fft3d_kernels_impl.cuh"
 #include "kern_registry.h"
 
+#include <set>
+#include <tuple>
+
 namespace fft3d {
+
+cudaError_t set_smem_attr(const void* func, int bytes) {
+  static std::mutex mu;
+  static std::set<std::tuple<const void*, int, int>> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_tuple(func, dev, bytes);
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count(key)) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) done.insert(key);
+  return e;
+}
 
 namespace {
 

@@ -8,6 +8,7 @@
 #include "fft3d_kernels.cuh"
 #include "kern_registry.h"
 #include "regfft.cuh"
+#include "fft3d_attr.h"
 
 namespace fft3d {
 namespace {
@@ -785,13 +786,13 @@ cudaError_t fwd_batch(const BatchLaunch& l, int bytes, cudaStream_t s) {
   const auto* args = static_cast<const ForwardArgs*>(l.args);
   cudaError_t e = cudaSuccess;
   if (bytes == 1) {
-    e = cudaFuncSetAttribute(k_forward_batch<BW, BH, uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    e = fft3d::smem_attr(k_forward_batch<BW, BH, uint8_t>, smem);
     if (e == cudaSuccess) k_forward_batch<BW, BH, uint8_t><<<l.grid, kWarps * 32, smem, s>>>(args, l.items, l.nitems);
   } else if (bytes == 2) {
-    e = cudaFuncSetAttribute(k_forward_batch<BW, BH, uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    e = fft3d::smem_attr(k_forward_batch<BW, BH, uint16_t>, smem);
     if (e == cudaSuccess) k_forward_batch<BW, BH, uint16_t><<<l.grid, kWarps * 32, smem, s>>>(args, l.items, l.nitems);
   } else {
-    e = cudaFuncSetAttribute(k_forward_batch<BW, BH, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    e = fft3d::smem_attr(k_forward_batch<BW, BH, float>, smem);
     if (e == cudaSuccess) k_forward_batch<BW, BH, float><<<l.grid, kWarps * 32, smem, s>>>(args, l.items, l.nitems);
   }
   return e != cudaSuccess ? e : cudaGetLastError();
@@ -800,8 +801,7 @@ cudaError_t fwd_batch(const BatchLaunch& l, int bytes, cudaStream_t s) {
 template <int BW, int BH, int MODE>
 cudaError_t inv_batch_mode(const BatchLaunch& l, cudaStream_t s) {
   const int smem = kWarps * fft_smem_bytes<BW, BH>();
-  cudaError_t e = cudaFuncSetAttribute(k_filter_inverse_batch<BW, BH, MODE>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = fft3d::smem_attr(k_filter_inverse_batch<BW, BH, MODE>, smem);
   if (e != cudaSuccess) return e;
   k_filter_inverse_batch<BW, BH, MODE><<<l.grid, kWarps * 32, smem, s>>>(static_cast<const InverseArgs*>(l.args),
                                                                          l.items, l.nitems);
@@ -856,13 +856,13 @@ cudaError_t fwd_sized(const ForwardArgs& a, int bytes, cudaStream_t s) {
   const int grid = fft_grid<BW, BH>(a.g.nblocks);
   cudaError_t e = cudaSuccess;
   if (bytes == 1) {
-    e = cudaFuncSetAttribute(k_forward<BW, BH, uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    e = fft3d::smem_attr(k_forward<BW, BH, uint8_t>, smem);
     if (e == cudaSuccess) k_forward<BW, BH, uint8_t><<<grid, kWarps * 32, smem, s>>>(a);
   } else if (bytes == 2) {
-    e = cudaFuncSetAttribute(k_forward<BW, BH, uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    e = fft3d::smem_attr(k_forward<BW, BH, uint16_t>, smem);
     if (e == cudaSuccess) k_forward<BW, BH, uint16_t><<<grid, kWarps * 32, smem, s>>>(a);
   } else {
-    e = cudaFuncSetAttribute(k_forward<BW, BH, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    e = fft3d::smem_attr(k_forward<BW, BH, float>, smem);
     if (e == cudaSuccess) k_forward<BW, BH, float><<<grid, kWarps * 32, smem, s>>>(a);
   }
   return e != cudaSuccess ? e : cudaGetLastError();
@@ -872,8 +872,7 @@ template <int BW, int BH, int MODE>
 cudaError_t inv_mode(const InverseArgs& a, cudaStream_t s) {
   constexpr int bulk_smem = 128 + kBulkWarps * bulk_warp_bytes<BW, BH, MODE>();
   if (MODE != MODE_KALMAN && a.bulk && a.err && bulk_smem <= 160 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_filter_inverse_bulk<BW, BH, MODE>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, bulk_smem);
+    cudaError_t e = fft3d::smem_attr(k_filter_inverse_bulk<BW, BH, MODE>, bulk_smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0, dev = 0, sms = 0;
     cudaGetDevice(&dev);
@@ -888,7 +887,7 @@ cudaError_t inv_mode(const InverseArgs& a, cudaStream_t s) {
   const int smem = kWarps * fft_smem_bytes<BW, BH>();
   const int grid = fft_grid<BW, BH>(a.g.nblocks);
   cudaError_t e =
-      cudaFuncSetAttribute(k_filter_inverse<BW, BH, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      fft3d::smem_attr(k_filter_inverse<BW, BH, MODE>, smem);
   if (e != cudaSuccess) return e;
   k_filter_inverse<BW, BH, MODE><<<grid, kWarps * 32, smem, s>>>(a);
   return cudaGetLastError();
@@ -900,7 +899,7 @@ cudaError_t fused_mode(const FusedArgs& a, cudaStream_t s) {
   const int smem = kFusedWarps * BH * (BW / 2 + 1) * 8 * (1 + NOLD);
   const int grid = (a.v.g.nblocks + kFusedWarps - 1) / kFusedWarps;
   cudaError_t e =
-      cudaFuncSetAttribute(k_fused<BW, BH, T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      fft3d::smem_attr(k_fused<BW, BH, T, MODE>, smem);
   if (e != cudaSuccess) return e;
   k_fused<BW, BH, T, MODE><<<grid, kFusedWarps * 32, smem, s>>>(a);
   return cudaGetLastError();

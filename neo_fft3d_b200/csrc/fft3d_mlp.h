@@ -35,6 +35,8 @@ cudaError_t colsum(const float* X, float* partial, float* out, long long rows, i
 cudaError_t adam(float* w, const float* g, float* m, float* v, void* wb, long long n, float lr, float b1, float b2,
                  float eps, int step, cudaStream_t s);
 cudaError_t to_bf16(const float* x, void* y, long long n, cudaStream_t s);
+// dst [cols][rows] = transpose of src [rows][cols] (BF16)
+cudaError_t transpose_bf16(const void* src, void* dst, int rows, int cols, cudaStream_t s);
 
 }  // namespace mlp
 }  // namespace fft3d

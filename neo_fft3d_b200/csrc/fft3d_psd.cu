@@ -469,6 +469,9 @@ struct fft3d::psd::Work {
   __nv_bfloat16 *H1 = nullptr, *H2 = nullptr;
   float *dY = nullptr, *dH = nullptr;
   __nv_bfloat16 *dYb = nullptr, *dZb = nullptr;
+  // transposed copies for the backward's K-major GEMMs: activations [features][rows], weights [in][out]
+  __nv_bfloat16 *dYbT = nullptr, *dZbT = nullptr, *H1T = nullptr, *H2T = nullptr, *XT = nullptr;
+  __nv_bfloat16 *W2T = nullptr, *W3T = nullptr;
   float* partial = nullptr;
   float* mean = nullptr;
 };
@@ -510,12 +513,19 @@ Work* work_alloc(long long rows, bool train) {
   const size_t oX = take(rows * IN * 2), oZ1 = take(rows * HID * 4), oZ2 = take(rows * HID * 4),
                oY = take(rows * OUT * 4), oH1 = take(rows * HID * 2), oH2 = take(rows * HID * 2),
                oP = take(fft3d::mlp::colsum_partial_floats(rows, OUT) * 4), oM = take(OUT * 4);
-  size_t odY = 0, odH = 0, odYb = 0, odZb = 0;
+  size_t odY = 0, odH = 0, odYb = 0, odZb = 0, odYbT = 0, odZbT = 0, oH1T = 0, oH2T = 0, oXT = 0, oW2T = 0, oW3T = 0;
   if (train) {
     odY = take(rows * OUT * 4);
     odH = take(rows * HID * 4);
     odYb = take(rows * OUT * 2);
     odZb = take(rows * HID * 2);
+    odYbT = take(rows * OUT * 2);
+    odZbT = take(rows * HID * 2);
+    oH1T = take(rows * HID * 2);
+    oH2T = take(rows * HID * 2);
+    oXT = take(rows * IN * 2);
+    oW2T = take((size_t)HID * HID * 2);
+    oW3T = take((size_t)HID * OUT * 2);
   }
   if (cudaMalloc(&w->mem, off) != cudaSuccess) {
     cudaGetLastError();
@@ -537,6 +547,13 @@ Work* work_alloc(long long rows, bool train) {
     w->dH = reinterpret_cast<float*>(b + odH);
     w->dYb = reinterpret_cast<__nv_bfloat16*>(b + odYb);
     w->dZb = reinterpret_cast<__nv_bfloat16*>(b + odZb);
+    w->dYbT = reinterpret_cast<__nv_bfloat16*>(b + odYbT);
+    w->dZbT = reinterpret_cast<__nv_bfloat16*>(b + odZbT);
+    w->H1T = reinterpret_cast<__nv_bfloat16*>(b + oH1T);
+    w->H2T = reinterpret_cast<__nv_bfloat16*>(b + oH2T);
+    w->XT = reinterpret_cast<__nv_bfloat16*>(b + oXT);
+    w->W2T = reinterpret_cast<__nv_bfloat16*>(b + oW2T);
+    w->W3T = reinterpret_cast<__nv_bfloat16*>(b + oW3T);
   }
   return w;
 }
@@ -559,19 +576,29 @@ cudaError_t backward(fft3d_psd* m, Work* w, const __nv_bfloat16* X, const float*
                      cudaStream_t s) {
   using namespace fft3d::mlp;
   const int R = (int)rows;
+  // every GEMM below reads both operands along K (the pipelined kernel); the
+  // operands that are not stored that way are transposed first
   CKE(mse_grad(w->Y, OUT, T, BINS, w->dY, w->dYb, rows, BINS, loss, s));
   // layer 3: dW3 = dY^T H2, db3 = colsum dY, dH2 = dY W3
-  CKE(gemm_bf16(w->dYb, 1, OUT, w->H2, 1, HID, m->g + O_W3, HID, OUT, HID, R, false, m->err, s));
+  CKE(transpose_bf16(w->dYb, w->dYbT, R, OUT, s));
+  CKE(transpose_bf16(w->H2, w->H2T, R, HID, s));
+  CKE(gemm_bf16(w->dYbT, R, 1, w->H2T, R, 1, m->g + O_W3, HID, OUT, HID, R, false, m->err, s));
   CKE(colsum(w->dY, w->partial, m->g + O_B3, rows, OUT, 1.f, s));
-  CKE(gemm_bf16(w->dYb, OUT, 1, m->wb + O_W3, 1, HID, w->dH, HID, R, HID, OUT, false, m->err, s));
+  CKE(transpose_bf16(m->wb + O_W3, w->W3T, OUT, HID, s));
+  CKE(gemm_bf16(w->dYb, OUT, 1, w->W3T, OUT, 1, w->dH, HID, R, HID, OUT, false, m->err, s));
   CKE(gelu_back(w->dH, w->Z2, w->dH, w->dZb, rows * HID, s));
   // layer 2
-  CKE(gemm_bf16(w->dZb, 1, HID, w->H1, 1, HID, m->g + O_W2, HID, HID, HID, R, false, m->err, s));
+  CKE(transpose_bf16(w->dZb, w->dZbT, R, HID, s));
+  CKE(transpose_bf16(w->H1, w->H1T, R, HID, s));
+  CKE(gemm_bf16(w->dZbT, R, 1, w->H1T, R, 1, m->g + O_W2, HID, HID, HID, R, false, m->err, s));
   CKE(colsum(w->dH, w->partial, m->g + O_B2, rows, HID, 1.f, s));
-  CKE(gemm_bf16(w->dZb, HID, 1, m->wb + O_W2, 1, HID, w->dH, HID, R, HID, HID, false, m->err, s));
+  CKE(transpose_bf16(m->wb + O_W2, w->W2T, HID, HID, s));
+  CKE(gemm_bf16(w->dZb, HID, 1, w->W2T, HID, 1, w->dH, HID, R, HID, HID, false, m->err, s));
   CKE(gelu_back(w->dH, w->Z1, w->dH, w->dZb, rows * HID, s));
   // layer 1
-  CKE(gemm_bf16(w->dZb, 1, HID, X, 1, IN, m->g + O_W1, IN, HID, IN, R, false, m->err, s));
+  CKE(transpose_bf16(w->dZb, w->dZbT, R, HID, s));
+  CKE(transpose_bf16(X, w->XT, R, IN, s));
+  CKE(gemm_bf16(w->dZbT, R, 1, w->XT, R, 1, m->g + O_W1, IN, HID, IN, R, false, m->err, s));
   CKE(colsum(w->dH, w->partial, m->g + O_B1, rows, HID, 1.f, s));
   return cudaSuccess;
 }

@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include "fft3d_kernels.cuh"
+#include "fft3d_attr.h"
 
 namespace fft3d {
 
@@ -396,14 +397,13 @@ cudaError_t launch_forward_tc(const ForwardArgs& a, const void* tables, int* err
   const uint8_t* t = static_cast<const uint8_t*>(tables);
   cudaError_t e = cudaSuccess;
   if (bytes == 1) {
-    e = cudaFuncSetAttribute(k_forward_tc<uint8_t, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_TC);
+    e = fft3d::smem_attr(k_forward_tc<uint8_t, false>, SMEM_TC);
     if (e == cudaSuccess) k_forward_tc<uint8_t, false><<<grid, THREADS, SMEM_TC, s>>>(a, t, err);
   } else if (bytes == 2) {
-    e = cudaFuncSetAttribute(k_forward_tc<uint16_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             SMEM_TC_SPLIT);
+    e = fft3d::smem_attr(k_forward_tc<uint16_t, true>, SMEM_TC_SPLIT);
     if (e == cudaSuccess) k_forward_tc<uint16_t, true><<<grid, THREADS, SMEM_TC_SPLIT, s>>>(a, t, err);
   } else {
-    e = cudaFuncSetAttribute(k_forward_tc<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_TC_SPLIT);
+    e = fft3d::smem_attr(k_forward_tc<float, true>, SMEM_TC_SPLIT);
     if (e == cudaSuccess) k_forward_tc<float, true><<<grid, THREADS, SMEM_TC_SPLIT, s>>>(a, t, err);
   }
   return e != cudaSuccess ? e : cudaGetLastError();
