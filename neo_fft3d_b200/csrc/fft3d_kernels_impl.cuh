@@ -14,7 +14,6 @@ namespace fft3d {
 namespace {
 
 constexpr int kWarps = 4;       // warps per CTA in k_forward / k_filter_inverse
-constexpr int kFusedWarps = 2;  // warps (= blocks) per CTA in k_fused
 
 // reflect-101 of index s into [0, n): the cover's mirror margins
 // (src/buffer.cpp:19-26, 65-79); repeated for planes narrower than a margin.
@@ -197,12 +196,6 @@ __device__ __forceinline__ void store_tdom(const float2* Sb, float* out, int lan
   }
 }
 
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // ---------------------------------------------------------------- forward
 
@@ -491,7 +484,9 @@ __host__ __device__ constexpr int fft_ctas(int nblocks) {
   return (nblocks + kWarps * blocks_per_warp<BW>() - 1) / (kWarps * blocks_per_warp<BW>());
 }
 
-template <int BW, int BH, int MODE>
+// NEWEST_IN_S: the window's newest frame (slot win_hi) is not read from
+// a.in[] but from S, where the fused kernel's forward transform left it.
+template <int BW, int BH, int MODE, bool NEWEST_IN_S = false>
 __device__ __forceinline__ void filter_inverse_cta(const InverseArgs& a, int vcta) {
   constexpr int NH = BW / 2 + 1, HC = BW / 2, NBW = blocks_per_warp<BW>(), BINS = BH * NH;
   constexpr int PER = (BINS + 31) / 32;
@@ -503,35 +498,48 @@ __device__ __forceinline__ void filter_inverse_cta(const InverseArgs& a, int vct
   const int blk0 = (cta * kWarps + warp) * NBW;
   if (blk0 >= g.nblocks) return;
   const float gs0 = __ldg(&a.t.grid[0].x);
-  constexpr int LO = win_lo<MODE>(), NW = win_hi<MODE>() - win_lo<MODE>() + 1;
+  constexpr int LO = win_lo<MODE>(), HI = win_hi<MODE>(), NW = HI - LO + 1;
+  constexpr int NG = NEWEST_IN_S ? NW - 1 : NW;  // window slots read from global memory
+  constexpr int NGB = NG > 0 ? NG : 1;
   // load-pipeline depth (chunks of 32 bins in flight): all chunks for a
   // one-frame window, fewer as the window (and the registers per chunk) grows
-  constexpr int DW = NW == 1 ? PER : (NW == 2 ? 10 : (NW == 3 ? 7 : (NW == 4 ? 5 : 4)));
+  constexpr int DW = NG <= 1 ? PER : (NG == 2 ? 10 : (NG == 3 ? 7 : (NG == 4 ? 5 : 4)));
   constexpr int D = PER < DW ? PER : DW;
 #pragma unroll 1
   for (int b = 0; b < NBW; b++) {
     const int blk = blk0 + b;
     if (blk >= g.nblocks) break;
     const size_t off = (size_t)blk * BINS;
-    const float gf = (MODE >= 1) ? a.c.degrid * __ldg(&a.in[2][off].x) / gs0 : 0.f;
+    float gf = 0.f;
+    if constexpr (MODE >= 1) {
+      if (NEWEST_IN_S && HI == 2) {
+        gf = a.c.degrid * S[b * BINS].x / gs0;
+        __syncwarp();  // every lane has the DC before lane 0 overwrites it
+      } else {
+        gf = a.c.degrid * __ldg(&a.in[2][off].x) / gs0;
+      }
+    }
     // software pipeline: the window's values of chunk j + D are loaded while
-    // chunk j is filtered, so D x NW loads per lane are always in flight
-    float2 buf[D][NW];
-    auto load = [&](int j, float2(&dst)[NW]) {
+    // chunk j is filtered, so D x NG loads per lane are always in flight
+    float2 buf[D][NGB];
+    auto load = [&](int j, float2(&dst)[NGB]) {
       const int i = lane + 32 * j;
 #pragma unroll
-      for (int k = 0; k < NW; k++) dst[k] = i < BINS ? __ldg(a.in[LO + k] + off + i) : make_float2(0.f, 0.f);
+      for (int k = 0; k < NG; k++) dst[k] = i < BINS ? __ldg(a.in[LO + k] + off + i) : make_float2(0.f, 0.f);
     };
+    if constexpr (NG > 0) {
 #pragma unroll
-    for (int j = 0; j < D; j++) load(j, buf[j]);
+      for (int j = 0; j < D; j++) load(j, buf[j]);
+    }
     float gsh = 0.f;
 #pragma unroll
     for (int j = 0; j < PER; j++) {
       const int i = lane + 32 * j;
       float2 w[5];
 #pragma unroll
-      for (int k = 0; k < 5; k++) w[k] = (k >= LO && k < LO + NW) ? buf[j % D][k - LO] : make_float2(0.f, 0.f);
-      if (j + D < PER) load(j + D, buf[j % D]);
+      for (int k = 0; k < 5; k++) w[k] = (k >= LO && k < LO + NG) ? buf[j % D][k - LO] : make_float2(0.f, 0.f);
+      if (NEWEST_IN_S && i < BINS) w[HI] = S[b * BINS + i];
+      if (NG > 0 && j + D < PER) load(j + D, buf[j % D]);
       float2 v = make_float2(0.f, 0.f);
       if (i < BINS) v = filter_vals<MODE>(a, w, off, i, gf, true);
       if (a.c.do_sharpen) {
@@ -696,80 +704,17 @@ __global__ void __launch_bounds__(kBulkWarps * 32) k_filter_inverse_bulk(Inverse
 
 // ---------------------------------------------------------------- fused
 
-// Steady-state hot path of one output frame: one warp per block
-//  0. cp.async copies of the older frames' spectra of the block into shared
-//     memory (they land while step 1 computes);
-//  1. forward transform of the window's newest frame (rows, columns) and its
-//     spectrum stored to the ring for the next output frames;
-//  2. filter of every bin (lane-consecutive bins), separate sharpen/dehalo pass;
-//  3. inverse transform (columns, rows) to the time-domain blocks.
+// Steady-state hot path of one output frame in one launch: each warp
+// transforms the window's newest frame for its blocks (forward_cta: the
+// spectra go to the ring for the next output frames and stay in the warp's
+// shared memory), then filters and inverse-transforms them
+// (filter_inverse_cta) with the older frames' spectra streamed from the ring
+// through the same register load pipeline as k_filter_inverse.
 template <int BW, int BH, typename T, int MODE>
-__global__ void __launch_bounds__(kFusedWarps * 32) k_fused(FusedArgs A) {
-  constexpr int NH = BW / 2 + 1, HC = BW / 2, BINS = BH * NH, PER = (BINS + 31) / 32;
-  constexpr int LO = win_lo<MODE>(), HI = win_hi<MODE>(), NOLD = HI - LO;
-  const InverseArgs& a = A.v;
-  const Geom& g = a.g;
-  extern __shared__ float2 smem2[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float2* S = smem2 + warp * BINS * (1 + NOLD);
-  float2* old = S + BINS;
-  const int cta = a.reverse ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
-  const int blk = cta * kFusedWarps + warp;
-  if (blk >= g.nblocks) return;
-  const size_t off = (size_t)blk * BINS;
-#pragma unroll
-  for (int q = 0; q < NOLD; q++) {
-    const float4* src = reinterpret_cast<const float4*>(a.in[LO + q] + off);
-    float4* dst = reinterpret_cast<float4*>(old + q * BINS);
-    for (int i = lane; i < BINS / 2; i += 32) cp_async16(dst + i, src + i);
-  }
-  cp_async_commit();
-  for (int y = lane; y < BH; y += 32) fwd_row<BW, BH, T>(A.f, blk, y, S);
-  __syncwarp();
-  for (int c = lane; c < HC; c += 32) fwd_col<BW, BH>(S, c);
-  __syncwarp();
-  {
-    float4* dst = reinterpret_cast<float4*>(A.f.spec + off);
-    const float4* src = reinterpret_cast<const float4*>(S);
-    for (int i = lane; i < BINS / 2; i += 32) dst[i] = src[i];
-  }
-  cp_async_wait_all();
-  __syncwarp();
-  const float gs0 = __ldg(&a.t.grid[0].x);
-  float gf = 0.f;
-  if constexpr (MODE >= 1) gf = a.c.degrid * (HI == 2 ? S[0].x : old[(2 - LO) * BINS].x) / gs0;
-  __syncwarp();  // every lane has read the DC before lane 0 rewrites it
-  float2 v[PER];
-#pragma unroll
-  for (int j = 0; j < PER; j++) {
-    const int i = lane + 32 * j;
-    if (i < BINS) {
-      float2 w[5];
-#pragma unroll
-      for (int k = 0; k < 5; k++)
-        w[k] = (k == HI) ? S[i] : ((k >= LO && k < HI) ? old[(k - LO) * BINS + i] : make_float2(0.f, 0.f));
-      v[j] = filter_vals<MODE>(a, w, off, i, gf, true);
-    }
-  }
-  if (a.c.do_sharpen) {
-    const float gsh = a.c.degrid * __shfl_sync(0xffffffffu, v[0].x, 0) / gs0;
-#pragma unroll
-    for (int j = 0; j < PER; j++) {
-      const int i = lane + 32 * j;
-      if (i < BINS) v[j] = sharpen_bin(a, v[j], i, gsh);
-    }
-  }
-#pragma unroll
-  for (int j = 0; j < PER; j++) {
-    const int i = lane + 32 * j;
-    if (i < BINS) S[i] = v[j];
-  }
-  __syncwarp();
-  for (int c = lane; c < HC; c += 32) inv_col<BW, BH>(S, c);
-  __syncwarp();
-  for (int y = lane; y < BH; y += 32) inv_row_inplace<BW, BH>(S, y);
-  __syncwarp();
-  store_tdom<BW, BH>(S, a.tdom + (size_t)blk * BH * BW, lane);
+__global__ void __launch_bounds__(kWarps * 32, 6) k_fused(FusedArgs A) {
+  const int n = fft_ctas<BW, BH>(A.v.g.nblocks);
+  forward_cta<BW, BH, T>(A.f, A.v.reverse ? n - 1 - (int)blockIdx.x : (int)blockIdx.x);
+  filter_inverse_cta<BW, BH, MODE, true>(A.v, blockIdx.x);
 }
 
 // ---------------------------------------------------------------- launchers
@@ -895,13 +840,12 @@ cudaError_t inv_mode(const InverseArgs& a, cudaStream_t s) {
 
 template <int BW, int BH, typename T, int MODE>
 cudaError_t fused_mode(const FusedArgs& a, cudaStream_t s) {
-  constexpr int NOLD = win_hi<MODE>() - win_lo<MODE>();
-  const int smem = kFusedWarps * BH * (BW / 2 + 1) * 8 * (1 + NOLD);
-  const int grid = (a.v.g.nblocks + kFusedWarps - 1) / kFusedWarps;
+  const int smem = kWarps * fft_smem_bytes<BW, BH>();
+  const int grid = fft_ctas<BW, BH>(a.v.g.nblocks);
   cudaError_t e =
       fft3d::smem_attr(k_fused<BW, BH, T, MODE>, smem);
   if (e != cudaSuccess) return e;
-  k_fused<BW, BH, T, MODE><<<grid, kFusedWarps * 32, smem, s>>>(a);
+  k_fused<BW, BH, T, MODE><<<grid, kWarps * 32, smem, s>>>(a);
   return cudaGetLastError();
 }
 
