@@ -89,10 +89,33 @@ struct fft3d_plane {
   float2* d_last = nullptr;
   float* d_cov = nullptr;
   float* d_covp = nullptr;
-  void* d_in = nullptr;   // staging of host frames (whole plane)
+  void* d_in = nullptr;   // staging of host frames (whole plane): the first stage's
   size_t in_pitch = 0;
-  void* d_out = nullptr;  // staging of the host output (whole plane)
+  void* d_out = nullptr;  // staging of the host output (whole plane): the first stage's
   size_t out_pitch = 0;
+  // Host path (fft3d_plane_filter): staging planes used round robin by the
+  // calls, uploads on s_up and downloads on s_down, ordered against the
+  // kernels on `stream` by events, so that the copies of one call overlap the
+  // kernels of another when the plane is called from several threads. The
+  // lock is held while a call is queued; the caller then waits on its own
+  // completion event.
+  struct Stage {
+    void* in = nullptr;
+    size_t in_pitch = 0;
+    void* out = nullptr;
+    size_t out_pitch = 0;
+    cudaEvent_t in_free = nullptr;   // the kernels reading `in` are done
+    cudaEvent_t out_free = nullptr;  // the download of `out` is done
+    int* h_flags = nullptr;          // pinned copies of the device error flags
+  };
+  static constexpr int kStages = 3;
+  Stage stages[kStages];
+  int next_stage = 0;
+  Stage* cur = nullptr;            // the stage of the call being queued
+  cudaEvent_t call_done = nullptr;  // completion event of the call being queued
+  cudaStream_t s_up = nullptr, s_down = nullptr;
+  std::mutex pool_mu;
+  std::vector<cudaEvent_t> sync_pool;
   uint64_t frames_done = 0;
   // kernel sequence of one output frame (NEO_FFT3D_PATH = unfused (default) | split | fused):
   //   split:   k_forward (new frame), k_filter_bins (streaming filter of all
@@ -268,8 +291,18 @@ void free_plane(fft3d_plane* P) {
   cudaFree(P->d_covp);
   cudaFree(P->d_psd);
   fft3d::psd::work_destroy(P->psd_work);
-  cudaFree(P->d_in);
-  cudaFree(P->d_out);
+  for (auto* st : {P->s_up, P->s_down})
+    if (st) cudaStreamSynchronize(st);
+  for (auto& sg : P->stages) {
+    cudaFree(sg.in);
+    cudaFree(sg.out);
+    if (sg.in_free) cudaEventDestroy(sg.in_free);
+    if (sg.out_free) cudaEventDestroy(sg.out_free);
+    if (sg.h_flags) cudaFreeHost(sg.h_flags);
+  }
+  for (auto e : P->sync_pool) cudaEventDestroy(e);
+  if (P->s_up) cudaStreamDestroy(P->s_up);
+  if (P->s_down) cudaStreamDestroy(P->s_down);
   if (P->stream) cudaStreamDestroy(P->stream);
   delete P;
 }
@@ -325,6 +358,45 @@ int launch_forward(fft3d_plane* P, const void* plane, long long stride, float2* 
   return FFT3D_OK;
 }
 
+cudaEvent_t take_sync_event(fft3d_plane* P) {
+  std::lock_guard<std::mutex> lk(P->pool_mu);
+  if (!P->sync_pool.empty()) {
+    cudaEvent_t e = P->sync_pool.back();
+    P->sync_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+  return e;
+}
+
+void give_sync_event(fft3d_plane* P, cudaEvent_t e) {
+  std::lock_guard<std::mutex> lk(P->pool_mu);
+  P->sync_pool.push_back(e);
+}
+
+// `wait` waits for the work queued so far on `done_on` (a stream-ordered
+// dependency; the event is free for reuse once the wait is queued).
+int stream_after(fft3d_plane* P, cudaStream_t wait, cudaStream_t done_on) {
+  cudaEvent_t e = take_sync_event(P);
+  CK(cudaEventRecord(e, done_on), "event");
+  CK(cudaStreamWaitEvent(wait, e, 0), "event");
+  give_sync_event(P, e);
+  return FFT3D_OK;
+}
+
+// Host path: the call's host frame into its staging plane, on the upload
+// stream, once the kernels that read the stage's previous frame are done;
+// the kernels of stream `st` then wait for the copy.
+int upload_frame(fft3d_plane* P, const void* plane, int stride, cudaStream_t st) {
+  fft3d_plane::Stage* sg = P->cur;
+  CK(cudaStreamWaitEvent(P->s_up, sg->in_free, 0), "event");
+  CK(cudaMemcpy2DAsync(sg->in, sg->in_pitch, plane, stride, (size_t)P->d.width * P->bytes, P->d.height,
+                       cudaMemcpyHostToDevice, P->s_up),
+     "frame upload");
+  return stream_after(P, st, P->s_up);
+}
+
 // The spectrum of frame m in a ring slot, computing it from `plane` if needed.
 int spectrum_slot(fft3d_plane* P, int m, int lo, int hi, const void* plane, int stride, bool host, cudaStream_t st,
                   Slot** out) {
@@ -337,13 +409,14 @@ int spectrum_slot(fft3d_plane* P, int m, int lo, int hi, const void* plane, int 
     const void* src = plane;
     long long sstride = stride;
     if (host) {
-      CK(cudaMemcpy2DAsync(P->d_in, P->in_pitch, plane, stride, (size_t)P->d.width * P->bytes, P->d.height,
-                           cudaMemcpyHostToDevice, st), "frame upload");
-      src = P->d_in;
-      sstride = (long long)P->in_pitch;
+      int rc = upload_frame(P, plane, stride, st);
+      if (rc) return rc;
+      src = P->cur->in;
+      sstride = (long long)P->cur->in_pitch;
     }
     int rc = launch_forward(P, src, sstride, s->spec, st);
     if (rc) return rc;
+    if (host) CK(cudaEventRecord(P->cur->in_free, st), "event");
     s->frame = m;
   }
   s->stamp = ++P->clock;
@@ -372,10 +445,13 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
   const void* cur = src ? src[2] : nullptr;
   if (bt == 0 && n == 0) {  // Kalman: frame 0 is returned unprocessed (:681-687)
     if (!cur) return fail(FFT3D_E_FRAME, "neo_fft3d: frame 0 was not supplied");
-    int rc = copy_plane(P, dst, dst_stride, cur, stride[2], host ? cudaMemcpyHostToHost : cudaMemcpyDeviceToDevice, st);
-    if (rc) return rc;
-    if (host) CK(cudaStreamSynchronize(st), "synchronize");
-    return FFT3D_OK;
+    if (host) {
+      for (int y = 0; y < P->d.height; y++)
+        std::memcpy(static_cast<char*>(dst) + (size_t)y * dst_stride, static_cast<const char*>(cur) + (size_t)y * stride[2],
+                    (size_t)P->d.width * P->bytes);
+      return FFT3D_OK;
+    }
+    return copy_plane(P, dst, dst_stride, cur, stride[2], cudaMemcpyDeviceToDevice, st);
   }
   if (P->pattern && !P->pattern_set)
     return fail(FFT3D_E_PARAM, "neo_fft3d: noise pattern not estimated yet (fft3d_plane_set_pattern_frame)");
@@ -415,10 +491,10 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
     new_src = plane;
     new_stride = stride[2 + to];
     if (host) {
-      CK(cudaMemcpy2DAsync(P->d_in, P->in_pitch, plane, stride[2 + to], (size_t)P->d.width * P->bytes, P->d.height,
-                           cudaMemcpyHostToDevice, st), "frame upload");
-      new_src = P->d_in;
-      new_stride = (long long)P->in_pitch;
+      int rc = upload_frame(P, plane, stride[2 + to], st);
+      if (rc) return rc;
+      new_src = P->cur->in;
+      new_stride = (long long)P->cur->in_pitch;
     }
     ia.in[2 + to] = news->spec;
   }
@@ -468,8 +544,11 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
       fft3d::FusedArgs fa;
       fa.f = forward_args(P, new_src, new_stride, news->spec);
       fa.v = ia;
-      TimeScope ts(P, K_FUSED, (double)P->g.W * P->g.H * P->bytes + (to - from) * S + S + state + T, st);
-      CK(fft3d::launch_fused(fa, mode, P->bytes, st), "fused kernel");
+      {
+        TimeScope ts(P, K_FUSED, (double)P->g.W * P->g.H * P->bytes + (to - from) * S + S + state + T, st);
+        CK(fft3d::launch_fused(fa, mode, P->bytes, st), "fused kernel");
+      }
+      if (host) CK(cudaEventRecord(P->cur->in_free, st), "event");
     } else if (P->path == 0 && mode != fft3d::MODE_SHARPEN_ONLY) {
       {
         // reads: the spectra of the window (+ Kalman state); writes: the filtered spectrum
@@ -501,8 +580,10 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
   void* odst = dst;
   long long ostride = dst_stride;
   if (host) {
-    odst = P->d_out;
-    ostride = (long long)P->out_pitch;
+    odst = P->cur->out;
+    ostride = (long long)P->cur->out_pitch;
+    // the stage's previous result must have been downloaded
+    CK(cudaStreamWaitEvent(st, P->cur->out_free, 0), "event");
     if (crop) {
       if (!cur) return fail(FFT3D_E_FRAME, "neo_fft3d: the current frame is needed for the crop borders");
       for (int y = 0; y < P->d.height; y++)
@@ -533,21 +614,40 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
     g_launches++;
   }
   if (host) {
+    // download on its own stream once the kernels are done; then the error
+    // flags; the caller waits on the call's completion event
+    fft3d_plane::Stage* sg = P->cur;
+    int rc = stream_after(P, P->s_down, st);
+    if (rc) return rc;
     char* hdst = static_cast<char*>(dst) + (size_t)P->t * dst_stride + (size_t)P->l * P->bytes;
-    const char* ddst = static_cast<const char*>(P->d_out) + P->t * P->out_pitch + (size_t)P->l * P->bytes;
-    CK(cudaMemcpy2DAsync(hdst, dst_stride, ddst, P->out_pitch, (size_t)P->g.W * P->bytes, P->g.H,
-                         cudaMemcpyDeviceToHost, st), "result download");
-    CK(cudaStreamSynchronize(st), "synchronize");
-    for (int* flagp : {P->d_err, learned ? fft3d::psd::err_flag(P->psd_model) : nullptr}) {
-      if (!flagp) continue;
-      int flag = 0;
-      CK(cudaMemcpy(&flag, flagp, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
-      if (flag) {
-        cudaMemset(flagp, 0, sizeof(int));
-        return fail(FFT3D_E_CUDA, (flag & 2) ? "neo_fft3d: bulk copy completion wait timed out"
-                                             : "neo_fft3d: tensor-core MMA completion wait timed out");
-      }
-    }
+    const char* ddst = static_cast<const char*>(sg->out) + P->t * sg->out_pitch + (size_t)P->l * P->bytes;
+    CK(cudaMemcpy2DAsync(hdst, dst_stride, ddst, sg->out_pitch, (size_t)P->g.W * P->bytes, P->g.H,
+                         cudaMemcpyDeviceToHost, P->s_down), "result download");
+    CK(cudaEventRecord(sg->out_free, P->s_down), "event");
+    sg->h_flags[0] = sg->h_flags[1] = 0;
+    CK(cudaMemcpyAsync(&sg->h_flags[0], P->d_err, sizeof(int), cudaMemcpyDeviceToHost, P->s_down), "error flag");
+    if (learned)
+      CK(cudaMemcpyAsync(&sg->h_flags[1], fft3d::psd::err_flag(P->psd_model), sizeof(int), cudaMemcpyDeviceToHost,
+                         P->s_down), "error flag");
+    P->call_done = take_sync_event(P);
+    CK(cudaEventRecord(P->call_done, P->s_down), "event");
+  }
+  return FFT3D_OK;
+}
+
+// Waits for a queued host-path call and reports a device error flag it saw.
+int finish_call(fft3d_plane* P, cudaEvent_t done, fft3d_plane::Stage* sg, bool learned) {
+  const cudaError_t e = cudaEventSynchronize(done);
+  give_sync_event(P, done);
+  if (e != cudaSuccess) return cuda_fail(e, "synchronize");
+  const int flags[2] = {sg->h_flags[0], sg->h_flags[1]};
+  for (int k = 0; k < 2; k++) {
+    const int flag = flags[k];
+    if (!flag) continue;
+    int* dflag = k == 0 ? P->d_err : (learned ? fft3d::psd::err_flag(P->psd_model) : nullptr);
+    if (dflag) cudaMemset(dflag, 0, sizeof(int));
+    return fail(FFT3D_E_CUDA, (flag & 2) ? "neo_fft3d: bulk copy completion wait timed out"
+                                         : "neo_fft3d: tensor-core MMA completion wait timed out");
   }
   return FFT3D_OK;
 }
@@ -720,6 +820,8 @@ int fft3d_plane_create(const fft3d_params* p, const fft3d_plane_desc* d, int dev
   if ((rc = ensure_twiddles(device))) return bail(rc);
   {
     cudaError_t e = cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&P->s_up, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&P->s_down, cudaStreamNonBlocking);
     if (e != cudaSuccess) return bail(cuda_fail(e, "stream create"));
   }
   // one table allocation: wan_x, wan_y, wsyn_xl/xr, wsyn_yl/yr, grid, wsharpen, wdehalo, pattern2d, pattern3d
@@ -783,9 +885,19 @@ int fft3d_plane_create(const fft3d_params* p, const fft3d_plane_desc* d, int dev
         cudaMalloc(&P->d_covp, P->spec_elems() * sizeof(float)) != cudaSuccess)
       return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (Kalman state)"));
   }
-  if (cudaMallocPitch(&P->d_in, &P->in_pitch, (size_t)d->width * P->bytes, d->height) != cudaSuccess ||
-      cudaMallocPitch(&P->d_out, &P->out_pitch, (size_t)d->width * P->bytes, d->height) != cudaSuccess)
-    return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (staging)"));
+  for (auto& sg : P->stages) {
+    if (cudaMallocPitch(&sg.in, &sg.in_pitch, (size_t)d->width * P->bytes, d->height) != cudaSuccess ||
+        cudaMallocPitch(&sg.out, &sg.out_pitch, (size_t)d->width * P->bytes, d->height) != cudaSuccess ||
+        cudaMallocHost(&sg.h_flags, 2 * sizeof(int)) != cudaSuccess)
+      return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (staging)"));
+    if (cudaEventCreateWithFlags(&sg.in_free, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&sg.out_free, cudaEventDisableTiming) != cudaSuccess)
+      return bail(fail(FFT3D_E_CUDA, "neo_fft3d: event creation failed"));
+  }
+  P->d_in = P->stages[0].in;
+  P->in_pitch = P->stages[0].in_pitch;
+  P->d_out = P->stages[0].out;
+  P->out_pitch = P->stages[0].out_pitch;
   *out = P;
   if ((rc = fft3d_plane_reset(P))) { *out = nullptr; return bail(rc); }
   return FFT3D_OK;
@@ -812,9 +924,32 @@ void fft3d_plane_destroy(fft3d_plane* P) { free_plane(P); }
 int fft3d_plane_filter(fft3d_plane* P, int n, const void* const src[5], const int src_stride[5], void* dst,
                        int dst_stride) {
   if (!P || !dst) return fail(FFT3D_E_PARAM, "neo_fft3d: null argument");
-  std::lock_guard<std::mutex> lk(P->mu);
-  CK(cudaSetDevice(P->device), "cudaSetDevice");
-  return run_filter(P, n, src, src_stride, dst, dst_stride, true, P->stream);
+  cudaEvent_t done = nullptr;
+  fft3d_plane::Stage* sg = nullptr;
+  bool learned = false;
+  {
+    std::lock_guard<std::mutex> lk(P->mu);
+    CK(cudaSetDevice(P->device), "cudaSetDevice");
+    sg = &P->stages[P->next_stage];
+    P->next_stage = (P->next_stage + 1) % fft3d_plane::kStages;
+    P->cur = sg;
+    P->call_done = nullptr;
+    const int rc = run_filter(P, n, src, src_stride, dst, dst_stride, true, P->stream);
+    done = P->call_done;
+    P->call_done = nullptr;
+    P->cur = nullptr;
+    learned = P->psd_model != nullptr;
+    if (rc) {
+      if (done) {
+        cudaEventSynchronize(done);
+        give_sync_event(P, done);
+      }
+      return rc;
+    }
+  }
+  if (!done) return FFT3D_OK;  // answered on the host (Kalman frame 0)
+  cudaSetDevice(P->device);
+  return finish_call(P, done, sg, learned);
 }
 
 int fft3d_plane_filter_device(fft3d_plane* P, int n, const void* const src[5], const int src_stride[5], void* dst,
@@ -857,6 +992,8 @@ int fft3d_plane_set_pattern_frame(fft3d_plane* P, const void* src, int stride) {
   std::lock_guard<std::mutex> lk(P->mu);
   if (!P->pattern) return FFT3D_OK;
   CK(cudaSetDevice(P->device), "cudaSetDevice");
+  // host-path calls still in flight may be using the first stage
+  for (auto* st : {P->s_up, P->stream, P->s_down}) CK(cudaStreamSynchronize(st), "synchronize");
   Slot* s = evict_slot(P, 1, 0);
   s->frame = -1;
   CK(cudaMemcpy2DAsync(P->d_in, P->in_pitch, src, stride, (size_t)P->d.width * P->bytes, P->d.height,

@@ -49,3 +49,44 @@ def test_path_matches_default_10bit(gpu, monkeypatch, variant):
     for r, g in zip(ref, got):
         d = np.abs(r.astype(int) - g.astype(int))
         assert d.max() <= 1 and np.mean(d == 0) >= 0.999
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kw", [dict(sigma=3.0, bt=5, sharpen=0.3), dict(sigma=2.0, bt=1, l=4, r=6)],
+                         ids=["wiener5", "wiener2d_crop"])
+def test_host_calls_from_threads(gpu, kw):
+    """fft3d_plane_filter called for different frames from several threads at
+    once (copies of one call overlap the kernels of another) gives the same
+    bytes as calling it frame by frame."""
+    import threading
+    from neo_fft3d_b200.params import make_params, plane_descs
+    planes = synth.make_clip(200, 144, 24, noise_sigma=5.0, seed=93)
+    F = planes[0].shape[0]
+    p = make_params(bw=32, bh=32, ow=16, oh=16, **kw)
+    descs = plane_descs([a.shape[1:] for a in planes], 8, F)
+    ref = engine.filter_clip(planes, bits=8, bw=32, bh=32, ow=16, oh=16, **kw)
+    for a, d, r in zip(planes, descs, ref):
+        e = engine.PlaneEngine(p, d)
+        out = np.zeros_like(a)
+        counter, lock, errors = [0], threading.Lock(), []
+
+        def work():
+            while True:
+                with lock:
+                    n = counter[0]
+                    counter[0] += 1
+                if n >= F:
+                    return
+                try:
+                    e.filter(n, [a[n + k] if 0 <= n + k < F else None for k in range(-2, 3)], out[n])
+                except Exception as ex:  # reported below
+                    errors.append(ex)
+
+        th = [threading.Thread(target=work) for _ in range(4)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        e.close()
+        assert not errors
+        assert np.array_equal(out, r)
