@@ -241,29 +241,16 @@ void gridsample(const std::vector<float>& wx, const std::vector<float>& wy, doub
     }
 }
 
-// FindPatternBlock / SetPattern (src/helper.cpp:46-132) on a host copy of
-// the spectrum of frame pframe.
-void estimate_pattern(fft3d_plane* P, const std::vector<float2>& spec) {
-  const int nh = P->g.nh, nb = P->g.bh * nh;
+// SetPattern (src/helper.cpp:92-132) from a host copy of the pattern block's
+// spectrum: pattern2d = |X - gridfraction * gridsample|^2 * pwin.
+void set_pattern_from_block(fft3d_plane* P, const float2* s) {
+  const int nb = P->g.bh * P->g.nh;
   const float* gs = P->h_grid.data();
-  auto power = [&](const float2* s, int i, float gcur) {
-    float c0 = s[i].x - gcur * gs[2 * i], c1 = s[i].y - gcur * gs[2 * i + 1];
-    return c0 * c0 + c1 * c1;
-  };
-  if (P->ep.px == 0 && P->ep.py == 0) {
-    float best = 1e15f;
-    for (int by = 2; by < P->g.noy - 2; by++)
-      for (int bx = 2; bx < P->g.nox - 2; bx++) {
-        const float2* s = spec.data() + ((size_t)by * P->g.nox + bx) * nb;
-        float gcur = P->ep.degrid * s[0].x / gs[0];
-        float acc = 0;
-        for (int i = 0; i < nb; i++) acc += power(s, i, gcur) * P->h_pwin[i];
-        if (acc < best) { P->ep.px = bx; P->ep.py = by; best = acc; }
-      }
+  const float gcur = P->ep.degrid * s[0].x / gs[0];
+  for (int i = 0; i < nb; i++) {
+    const float c0 = s[i].x - gcur * gs[2 * i], c1 = s[i].y - gcur * gs[2 * i + 1];
+    P->h_pattern2d[i] = (c0 * c0 + c1 * c1) * P->h_pwin[i];
   }
-  const float2* s = spec.data() + ((size_t)P->ep.py * P->g.nox + P->ep.px) * nb;
-  float gcur = P->ep.degrid * s[0].x / gs[0];
-  for (int i = 0; i < nb; i++) P->h_pattern2d[i] = power(s, i, gcur) * P->h_pwin[i];
 }
 
 int ensure_twiddles(int dev) {
@@ -1000,11 +987,41 @@ int fft3d_plane_set_pattern_frame(fft3d_plane* P, const void* src, int stride) {
                        cudaMemcpyHostToDevice, P->stream), "frame upload");
   int rc = launch_forward(P, P->d_in, (long long)P->in_pitch, s->spec, P->stream);
   if (rc) return rc;
-  std::vector<float2> spec(P->spec_elems());
-  CK(cudaMemcpyAsync(spec.data(), s->spec, spec.size() * sizeof(float2), cudaMemcpyDeviceToHost, P->stream),
-     "spectrum download");
+  const int nb = P->g.bh * P->g.nh;
+  if (P->ep.px == 0 && P->ep.py == 0) {
+    // FindPatternBlock (src/helper.cpp:46-90): the interior block with the least
+    // windowed power, scored on the device in the reference's summation order;
+    // the first minimum in raster order wins, as in the reference's loop
+    const int wx = P->g.nox - 4, wy = P->g.noy - 4;
+    if (wx > 0 && wy > 0) {
+      float* d_buf = nullptr;
+      CK(cudaMalloc(&d_buf, ((size_t)wx * wy + nb) * sizeof(float)), "pattern scores");
+      std::vector<float> scores((size_t)wx * wy);
+      cudaError_t e = cudaMemcpyAsync(d_buf + (size_t)wx * wy, P->h_pwin.data(), nb * sizeof(float),
+                                      cudaMemcpyHostToDevice, P->stream);
+      if (e == cudaSuccess)
+        e = fft3d::launch_pattern_scores(s->spec, P->tab.grid, d_buf + (size_t)wx * wy, P->g.nox, P->g.noy, nb,
+                                         P->ep.degrid, d_buf, P->stream);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(scores.data(), d_buf, scores.size() * sizeof(float), cudaMemcpyDeviceToHost, P->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(P->stream);
+      cudaFree(d_buf);
+      if (e != cudaSuccess) return cuda_fail(e, "pattern scores");
+      float best = 1e15f;
+      for (size_t k = 0; k < scores.size(); k++)
+        if (scores[k] < best) {
+          best = scores[k];
+          P->ep.px = 2 + (int)(k % wx);
+          P->ep.py = 2 + (int)(k / wx);
+        }
+    }
+  }
+  std::vector<float2> blk(nb);
+  CK(cudaMemcpyAsync(blk.data(), s->spec + ((size_t)P->ep.py * P->g.nox + P->ep.px) * nb, nb * sizeof(float2),
+                     cudaMemcpyDeviceToHost, P->stream),
+     "pattern block download");
   CK(cudaStreamSynchronize(P->stream), "synchronize");
-  estimate_pattern(P, spec);
+  set_pattern_from_block(P, blk.data());
   rc = upload_pattern(P, P->d_pattern2d, P->h_pattern2d, P->stream);
   if (rc) return rc;
   CK(cudaStreamSynchronize(P->stream), "synchronize");

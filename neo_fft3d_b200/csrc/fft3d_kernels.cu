@@ -219,6 +219,33 @@ cudaError_t launch_copy_batch(const BatchLaunch& l, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+__global__ void __launch_bounds__(128) k_pattern_scores(const float2* __restrict__ spec,
+                                                        const float2* __restrict__ grid,
+                                                        const float* __restrict__ pwin, int nox, int noy,
+                                                        int bins, float degrid, float* scores) {
+  const int wx = nox - 4, wy = noy - 4;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= wx * wy) return;
+  const int by = 2 + i / wx, bx = 2 + i % wx;
+  const float2* s = spec + ((size_t)by * nox + bx) * bins;
+  const float gcur = __fdiv_rn(__fmul_rn(degrid, s[0].x), grid[0].x);
+  float acc = 0.f;
+  for (int k = 0; k < bins; k++) {
+    const float2 v = s[k], gs = grid[k];
+    const float c0 = __fsub_rn(v.x, __fmul_rn(gcur, gs.x)), c1 = __fsub_rn(v.y, __fmul_rn(gcur, gs.y));
+    acc = __fadd_rn(acc, __fmul_rn(__fadd_rn(__fmul_rn(c0, c0), __fmul_rn(c1, c1)), pwin[k]));
+  }
+  scores[i] = acc;
+}
+
+cudaError_t launch_pattern_scores(const float2* spec, const float2* grid, const float* pwin, int nox, int noy,
+                                  int bins, float degrid, float* scores, cudaStream_t s) {
+  const int n = (nox - 4) * (noy - 4);
+  if (n <= 0) return cudaSuccess;
+  k_pattern_scores<<<(n + 127) / 128, 128, 0, s>>>(spec, grid, pwin, nox, noy, bins, degrid, scores);
+  return cudaGetLastError();
+}
+
 int batch_items_forward(const Geom& g) {
   const SizeEntry* e = find_size(g.bw, g.bh);
   return e ? e->ctas(g.nblocks) : 0;

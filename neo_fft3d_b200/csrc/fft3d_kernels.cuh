@@ -150,6 +150,12 @@ cudaError_t launch_filter_bins(const InverseArgs& a, float2* F, int mode, cudaSt
 // cudaErrorNotSupported when no fused kernel exists for the sample type (float)
 cudaError_t launch_fused(const FusedArgs& a, int mode, int bytes_per_sample, cudaStream_t s);
 bool block_size_supported(int bw, int bh);
+// FindPatternBlock scores (src/helper.cpp:46-90): scores[(by-2)*(nox-4) + bx-2] =
+// sum over bins of |X - gridfraction * grid|^2 * pwin for the interior blocks
+// 2 <= bx < nox-2, 2 <= by < noy-2, accumulated bin by bin with every product
+// and sum rounded separately, as the reference's C loop.
+cudaError_t launch_pattern_scores(const float2* spec, const float2* grid, const float* pwin, int nox, int noy,
+                                  int bins, float degrid, float* scores, cudaStream_t s);
 cudaError_t upload_twiddles();  // every registered size, on the current device
 
 // Tensor-core forward transform of 32x32 blocks (fft3d_tc.cu): DFT tables for
