@@ -78,16 +78,22 @@ def main():
     ap.add_argument("--seed", type=int, default=400)
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--train-only", action="store_true", help="report the training measurements only")
+    ap.add_argument("--blocks", type=int, default=0, help="training blocks (0: library default)")
     args = ap.parse_args()
 
     m = psd.PsdModel(seed=1)
     t = time.perf_counter()
-    curve, val = m.train()
+    curve, val = m.train(**({"blocks": args.blocks} if args.blocks else {}))
     wall = time.perf_counter() - t
     st = m.train_stats()
     train = dict(wall_s=wall, held_out_loss=val, first_loss=float(curve[0]), last_loss=float(curve[-1]), **st,
                  gemm_tflops=st["gemm_flops_per_step"] * st["steps"] / (st["train_ms"] / 1000.0) / 1e12,
-                 blocks_per_s_generated=(psd.train_cfg().blocks + 32768) / (st["generate_ms"] / 1000.0))
+                 blocks_per_s_generated=((args.blocks or psd.train_cfg().blocks) + 32768) / (st["generate_ms"] / 1000.0))
+    if args.train_only:
+        print(json.dumps(dict(train=train)), flush=True)
+        m.close()
+        return
 
     rng = np.random.default_rng(args.seed)
     clips = []
