@@ -13,7 +13,7 @@
 
 namespace fft3d {
 
-cudaError_t set_smem_attr(const void* func, int bytes) {
+cudaError_t set_smem_attr(const void* func, int bytes, bool prefer_shared) {
   static std::mutex mu;
   static std::set<std::tuple<const void*, int, int>> done;
   int dev = 0;
@@ -21,7 +21,9 @@ cudaError_t set_smem_attr(const void* func, int bytes) {
   const auto key = std::make_tuple(func, dev, bytes);
   std::lock_guard<std::mutex> lk(mu);
   if (done.count(key)) return cudaSuccess;
-  const cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess && prefer_shared)
+    e = cudaFuncSetAttribute(func, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e == cudaSuccess) done.insert(key);
   return e;
 }

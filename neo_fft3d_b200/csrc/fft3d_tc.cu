@@ -397,13 +397,13 @@ cudaError_t launch_forward_tc(const ForwardArgs& a, const void* tables, int* err
   const uint8_t* t = static_cast<const uint8_t*>(tables);
   cudaError_t e = cudaSuccess;
   if (bytes == 1) {
-    e = fft3d::smem_attr(k_forward_tc<uint8_t, false>, SMEM_TC);
+    e = fft3d::smem_attr(k_forward_tc<uint8_t, false>, SMEM_TC, true);
     if (e == cudaSuccess) k_forward_tc<uint8_t, false><<<grid, THREADS, SMEM_TC, s>>>(a, t, err);
   } else if (bytes == 2) {
-    e = fft3d::smem_attr(k_forward_tc<uint16_t, true>, SMEM_TC_SPLIT);
+    e = fft3d::smem_attr(k_forward_tc<uint16_t, true>, SMEM_TC_SPLIT, true);
     if (e == cudaSuccess) k_forward_tc<uint16_t, true><<<grid, THREADS, SMEM_TC_SPLIT, s>>>(a, t, err);
   } else {
-    e = fft3d::smem_attr(k_forward_tc<float, true>, SMEM_TC_SPLIT);
+    e = fft3d::smem_attr(k_forward_tc<float, true>, SMEM_TC_SPLIT, true);
     if (e == cudaSuccess) k_forward_tc<float, true><<<grid, THREADS, SMEM_TC_SPLIT, s>>>(a, t, err);
   }
   return e != cudaSuccess ? e : cudaGetLastError();

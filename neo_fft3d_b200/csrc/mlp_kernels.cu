@@ -404,7 +404,7 @@ template <int BN>
 cudaError_t launch_pipe(const __nv_bfloat16* A, long long lda, const __nv_bfloat16* B, long long ldb, float* C,
                         long long ldc, int M, int N, int K, bool accumulate, int* err, cudaStream_t s) {
   constexpr int smem = PipeCfg<BN>::SMEM;
-  cudaError_t e = fft3d::smem_attr(k_gemm_pipe<BN>, smem);
+  cudaError_t e = fft3d::smem_attr(k_gemm_pipe<BN>, smem, true);
   if (e != cudaSuccess) return e;
   k_gemm_pipe<BN><<<dim3(N / BN, M / PM), 128, smem, s>>>(A, lda, B, ldb, C, ldc, K, accumulate ? 1 : 0, err);
   return cudaGetLastError();
