@@ -12,9 +12,11 @@ in HBM. The clip (373 MB) and the spectrum ring (~350 MB) are larger than L2,
 so no flush is needed between steps.
 
 Both forms of the block transform run K timed steps each: the plain FP32
-register FFT (as three kernels per plane-frame, and fused into two) and the
-tensor-core split-precision BF16 DFT-GEMM (32x32 blocks); their outputs are
-compared pixel by pixel (within +-1 LSB).
+register FFT (as three kernels per plane-frame, fused into two, and in frame
+groups of FRAME_GROUP consecutive frames per call, whose filter/inverse is one
+launch) and the tensor-core split-precision BF16 DFT-GEMM (32x32 blocks); their
+outputs are compared pixel by pixel (within +-1 LSB; the fused and grouped
+forms byte for byte against the plain one).
 
 Lines printed (rank 0, one JSON line):
   value      frames/s of the faster form, device-resident (whole job over N ranks)
@@ -51,8 +53,11 @@ WORKLOAD = "1080p_bt5_bw32"
 METRIC = "1080p bt=5 frames/s: TC split-precision vs plain FP32 kernel at \u00b11 LSB; %HBM roofline"
 UNIT = "frames/s"
 # the two forms of the block transform that the metric compares (NEO_FFT3D_PATH)
-PATHS = {"plain_fp32": "unfused", "plain_fp32_fused": "fused", "tc_split_bf16": "tc"}
-PLAIN = ("plain_fp32", "plain_fp32_fused")
+PATHS = {"plain_fp32": "unfused", "plain_fp32_fused": "fused", "plain_fp32_frames": "unfused",
+         "tc_split_bf16": "tc"}
+PLAIN = ("plain_fp32", "plain_fp32_fused", "plain_fp32_frames")
+# output frames per call of the grouped arm (fft3d_plane_filter_frames_device)
+FRAME_GROUP = 8
 
 
 def workload():
@@ -241,6 +246,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-kalman", action="store_true")
+    ap.add_argument("--arms", default=",".join(PATHS),
+                    help="comma-separated subset of the timed arms (profiling runs); the comparisons need all")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -274,30 +281,41 @@ def main():
     dev = [torch.from_numpy(a).cuda() for a in planes]
     master = torch.cuda.current_stream()
 
-    def make_arm(path):
+    def make_arm(path, group=0):
         os.environ["NEO_FFT3D_PATH"] = path
         engs = [engine.PlaneEngine(p, d, local) for d in descs]
         outs = [torch.empty_like(d) for d in dev]
         streams = [torch.cuda.Stream() for _ in engs]
 
+        def frames(i, lo, hi, s):
+            """Output frames [lo, hi) of plane i on stream s."""
+            e, a, o = engs[i], dev[i], outs[i]
+            W = a.shape[2]
+            fb = a.shape[1] * W
+            base = a.data_ptr()
+            obase = o.data_ptr()
+            if group:
+                for n0 in range(lo, hi, group):
+                    k = min(group, hi - n0)
+                    ptrs = [base + n * fb if 0 <= n < F else 0 for n in range(n0 - 2, n0 + k + 2)]
+                    e.filter_frames_device(n0, ptrs, [W] * (k + 4), [obase + n * fb for n in range(n0, n0 + k)],
+                                           [W] * k, s.cuda_stream)
+                return
+            for n in range(lo, hi):
+                ptrs = [base + (n + d) * fb if 0 <= n + d < F else 0 for d in range(-2, 3)]
+                e.filter_device(n, ptrs, [W] * 5, obase + n * fb, W, s.cuda_stream)
+
         def step(serial=False):
             ev = torch.cuda.Event()
             ev.record(master)
-            for i, e in enumerate(engs):
+            for i in range(len(engs)):
                 s = master if serial else streams[i]
                 s.wait_event(ev)
-                a, o = dev[i], outs[i]
-                W = a.shape[2]
-                fb = a.shape[1] * W
-                base = a.data_ptr()
-                obase = o.data_ptr()
-                for n in range(F):
-                    ptrs = [base + (n + d) * fb if 0 <= n + d < F else 0 for d in range(-2, 3)]
-                    e.filter_device(n, ptrs, [W] * 5, obase + n * fb, W, s.cuda_stream)
+                frames(i, 0, F, s)
             for s in streams:
                 master.wait_stream(s)
 
-        return {"engs": engs, "outs": outs, "step": step}
+        return {"engs": engs, "outs": outs, "step": step, "frames": frames, "group": group}
 
     def time_arm(arm):
         for _ in range(args.warmup):
@@ -323,7 +341,12 @@ def main():
         arm["ms"] = ms
         arm["value"] = world * F * args.steps / (ms / 1000.0)
 
-    arms = {name: make_arm(path) for name, path in PATHS.items()}
+    chosen = [a for a in args.arms.split(",") if a]
+    for a in chosen:
+        if a not in PATHS:
+            raise SystemExit(f"unknown arm {a}; arms: {', '.join(PATHS)}")
+    arms = {name: make_arm(path, FRAME_GROUP if name == "plain_fp32_frames" else 0)
+            for name, path in PATHS.items() if name in chosen}
     os.environ["NEO_FFT3D_PATH"] = PATHS["plain_fp32"]
     clocks = ClockSampler(local)
     clocks.start()
@@ -337,35 +360,49 @@ def main():
     value = head["value"]
     ms_per_step = head["ms"] / args.steps
     launches = head["launches"]
-    # the two forms' outputs (the last step wrote every frame of every plane)
-    diff_max, within, total_px = 0, 0, 0
-    for a, b in zip(arms["plain_fp32"]["outs"], arms["tc_split_bf16"]["outs"]):
-        d = (a.to(torch.int16) - b.to(torch.int16)).abs()
-        diff_max = max(diff_max, int(d.max().item()))
-        within += int((d <= 1).sum().item())
-        total_px += d.numel()
     paths = {name: {"value": arm["value"], "ms_per_step": arm["ms"] / args.steps, "launches": arm["launches"],
                     "NEO_FFT3D_PATH": PATHS[name]} for name, arm in arms.items()}
-    best_plain = max(arms[k]["value"] for k in PLAIN)
-    paths["tc_over_plain"] = arms["tc_split_bf16"]["value"] / best_plain
-    # the fused sequence against the unfused one (same FP32 arithmetic)
-    fd_max, fd_within = 0, 0
-    for a, b in zip(arms["plain_fp32"]["outs"], arms["plain_fp32_fused"]["outs"]):
-        d = (a.to(torch.int16) - b.to(torch.int16)).abs()
-        fd_max = max(fd_max, int(d.max().item()))
-        fd_within += int((d <= 1).sum().item())
-    paths["fused_vs_unfused_output"] = {"within_1lsb": fd_within / total_px, "max_abs_diff": fd_max}
-    paths["tc_vs_plain_output"] = {"within_1lsb": within / total_px, "max_abs_diff": diff_max, "pixels": total_px}
+    if len(arms) == len(PATHS):
+        # the two forms' outputs (the last step wrote every frame of every plane)
+        diff_max, within, total_px = 0, 0, 0
+        for a, b in zip(arms["plain_fp32"]["outs"], arms["tc_split_bf16"]["outs"]):
+            d = (a.to(torch.int16) - b.to(torch.int16)).abs()
+            diff_max = max(diff_max, int(d.max().item()))
+            within += int((d <= 1).sum().item())
+            total_px += d.numel()
+        best_plain = max(arms[k]["value"] for k in PLAIN)
+        paths["tc_over_plain"] = arms["tc_split_bf16"]["value"] / best_plain
+        # the fused sequence against the unfused one (same FP32 arithmetic)
+        fd_max, fd_within = 0, 0
+        for a, b in zip(arms["plain_fp32"]["outs"], arms["plain_fp32_fused"]["outs"]):
+            d = (a.to(torch.int16) - b.to(torch.int16)).abs()
+            fd_max = max(fd_max, int(d.max().item()))
+            fd_within += int((d <= 1).sum().item())
+        paths["fused_vs_unfused_output"] = {"within_1lsb": fd_within / total_px, "max_abs_diff": fd_max}
+        # frame groups run the unfused kernels' arithmetic: byte-identical
+        paths["frames_vs_unfused_output"] = {
+            "identical": all(bool(torch.equal(a, b)) for a, b in zip(arms["plain_fp32"]["outs"],
+                                                                       arms["plain_fp32_frames"]["outs"])),
+            "frames_per_call": FRAME_GROUP}
+        paths["tc_vs_plain_output"] = {"within_1lsb": within / total_px, "max_abs_diff": diff_max,
+                                       "pixels": total_px}
 
     # per-kernel roofline from an instrumented pass (events around each
     # launch; planes serialised on one stream so that no other kernel shares
     # the GPU during a timed launch). The dominant kernel is taken on the luma
     # plane, whose launches are the largest.
+    # Each chunk of frames is queued while the GPU waits in a sleep kernel, so
+    # that the events around a launch bracket the kernel alone and not the
+    # host's time to issue it.
     for e in engs:
         e.set_timing(True)
-    for _ in range(3):
-        step(serial=True)
-    torch.cuda.synchronize()
+    chunk = max(head["group"], 1) * max(1, 8 // max(head["group"], 1))
+    for _ in range(2):
+        for i in range(len(engs)):
+            for lo in range(0, F, chunk):
+                torch.cuda._sleep(2_000_000)
+                head["frames"](i, lo, min(lo + chunk, F), master)
+            torch.cuda.synchronize()
     per_plane = [e.timing() for e in engs]
     for e in engs:
         e.set_timing(False)
@@ -374,7 +411,10 @@ def main():
     n_l, ms_l, b_l = per_plane[0][dom]
     peak, peak_kind = load_peaks()
     achieved = (b_l / n_l) / (ms_l / n_l / 1000.0) / 1e9
-    traffic = load_traffic().get(dom)
+    traffic = load_traffic().get(f"{dom}_frames{head['group']}" if head["group"] else dom)
+    if isinstance(traffic, dict):
+        # captured on one launch; scaled to the average launch by algorithmic bytes
+        traffic = traffic["traffic"] * (b_l / n_l) / traffic["algorithmic"]
     share_den = sum(total_ms.values())
     roofline = {"bound": "hbm", "kernel": dom, "plane": "luma", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind,
@@ -383,8 +423,17 @@ def main():
                 "kernel_share": {k: v / share_den for k, v in total_ms.items() if v > 0}}
     nblocks_total = sum(e.nblocks for e in engs)
     fb_bytes = canonical_frame_bytes(clip_kw["width"], clip_kw["height"], nblocks_total, p.bh, p.bw // 2 + 1, p.bt)
-    frame_roofline = {"bytes_per_frame": fb_bytes, "achieved_gbs": fb_bytes * value / world / 1e9,
+    frame_roofline = {"model": "cached spectra, one output frame at a time: P_in + S + bt*S + P_out",
+                      "bytes_per_frame": fb_bytes, "achieved_gbs": fb_bytes * value / world / 1e9,
                       "frac": fb_bytes * value / world / 1e9 / peak}
+    if head["group"]:
+        # a frame group of G frames reads the G + bt - 1 window spectra once
+        G = head["group"]
+        S_all = nblocks_total * p.bh * (p.bw // 2 + 1) * 8
+        gb = fb_bytes - p.bt * S_all + (G + p.bt - 1) / G * S_all
+        frame_roofline["head_path_model"] = {
+            "model": f"frame groups of {G}: P_in + S + (G + bt - 1)/G * S + P_out",
+            "bytes_per_frame": gb, "achieved_gbs": gb * value / world / 1e9, "frac": gb * value / world / 1e9 / peak}
 
     # end to end through the C ABI with pinned host buffers (one host thread per plane)
     host_in = [torch.from_numpy(a).pin_memory() for a in planes]
@@ -463,7 +512,7 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "frames_per_step": F, "width": 1920, "height": 1080,
                        "format": "YUV420P8", "bt": 5, "sigma": 3.0, "bw": 32, "bh": 32, "ow": 16, "oh": 16,
-                       "sharpen": 0.3, "path": head_name,
+                       "sharpen": 0.3, "path": head_name, "frames_per_call": head["group"] or 1,
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (373 MB clip + ~350 MB spectrum ring per rank), no flush"},
             "roofline": roofline, "frame_roofline": frame_roofline, "cpu_baseline": cpu, "e2e": e2e,

@@ -90,6 +90,25 @@ int fft3d_plane_filter(fft3d_plane* h, int n, const void* const src[5], const in
 int fft3d_plane_filter_device(fft3d_plane* h, int n, const void* const src[5], const int src_stride[5], void* dst,
                               int dst_stride, void* stream);
 
+/* Frame group (no counterpart in the reference, whose engine filters one
+ * output frame per GetFrame, src/fft3d_engine.h:452-734): output frames
+ * n0 .. n0 + count - 1 of one plane in one call, 1 <= count <=
+ * FFT3D_MAX_FRAME_GROUP. DEVICE pointers: src[j] is frame n0 - 2 + j for
+ * j in [0, count + 4) with stride src_stride[j] (NULL outside the clip, or
+ * where the frame's spectrum is cached); frame n0 + j is written to dst[j]
+ * (stride dst_stride[j]); all work is queued on `stream` (NULL = the
+ * handle's own stream). On the default path, Wiener 3D planes (bt = 2..5)
+ * filter the group's frames with one filter/inverse launch whose CTAs
+ * interleave the frames block range by block range, so that a window
+ * spectrum shared by up to bt frames is read from HBM about once; the ring
+ * keeps every spectrum the group needs and there is one time-domain buffer
+ * per frame (both grow on first use: count + bt spectra and count - 1
+ * buffers). Other planes filter the frames one after another. Outputs are
+ * those of count calls of fft3d_plane_filter_device. */
+#define FFT3D_MAX_FRAME_GROUP 16
+int fft3d_plane_filter_frames_device(fft3d_plane* h, int n0, int count, const void* const* src,
+                                     const int* src_stride, void* const* dst, const int* dst_stride, void* stream);
+
 /* 1 if the spectrum of frame n is held in the device spectrum cache. */
 int fft3d_plane_cached(fft3d_plane* h, int n);
 
@@ -177,7 +196,15 @@ int fft3d_batch_set_tuning(fft3d_batch* b, int enable);
  * is queued on `stream` (a cudaStream_t) without a host synchronisation
  * (except while a new step shape is tuned). Successive steps of one batch
  * must use one stream. Planes must be on the batch's device, on the default
- * (unfused) path, without a learned PSD; each plane at most once per step. */
+ * (unfused) path, without a learned PSD.
+ * Frame groups: a Wiener/sharpen plane (bt != 0) may appear several times in
+ * one step with consecutive frames n, n + 1, ... (in item order). The
+ * group's filter/inverse work items then run together, interleaved frame by
+ * frame over the same blocks, so that each block's window spectra are read
+ * from HBM about once per group instead of once per frame (the rest hit L2);
+ * the plane keeps every spectrum the group needs (its ring and time-domain
+ * buffers grow on first use). Outputs are those of one-frame-at-a-time
+ * filtering. A Kalman plane (bt = 0) appears at most once per step. */
 int fft3d_batch_step(fft3d_batch* b, int count, fft3d_plane* const* planes, const int* n, const void* const* src,
                      const int* src_stride, void* const* dst, const int* dst_stride, void* stream);
 
@@ -185,6 +212,15 @@ int fft3d_batch_step(fft3d_batch* b, int count, fft3d_plane* const* planes, cons
  * of the last step, [5] step shapes seen, [6] wave budget (MiB, 0 = one
  * wave) of the last tuned step, [7] 0. */
 int fft3d_batch_stats(fft3d_batch* b, double out[8]);
+
+/* Per-phase kernel timing (1 = on). While on, tuned steps run without their
+ * CUDA graph, with events around every launch. fft3d_batch_timing waits for
+ * the timed launches and returns, cumulated since the batch was created,
+ * out[3*k + 0] launches, [3*k + 1] milliseconds and [3*k + 2] algorithmic
+ * bytes (each distinct input read once, outputs written once) for k = 0
+ * forward, 1 filter/inverse, 2 plane copies, 3 overlap-add. */
+int fft3d_batch_set_timing(fft3d_batch* b, int enable);
+int fft3d_batch_timing(fft3d_batch* b, double out[12]);
 
 /* ------------------------------------------------------------------------
  * Learned noise PSD. No counterpart in the reference, whose per-frequency

@@ -162,6 +162,16 @@ struct fft3d_batch {
   cudaEvent_t direct_done = nullptr;
   double stats[8] = {};  // steps, graph launches, tuning steps, -, kernels of the last step, step shapes,
                          // wave budget (MiB) of the last tuned step
+  // optional per-phase timing: tuned steps run without the graph, with
+  // events around each launch, resolved when the counters are read
+  struct Pending {
+    int phase;
+    double bytes;
+    cudaEvent_t a, b;
+  };
+  bool timing = false;
+  std::vector<Pending> pending;
+  double t_phase[4][3] = {};  // launches, ms, algorithmic bytes
 };
 
 namespace {
@@ -283,6 +293,44 @@ void write_items(const Plan& plan, char* base) {  // base: start of the items ar
   }
 }
 
+// Algorithmic bytes of one group's launch: what its records must read and
+// write at least. Filter/inverse: each distinct window spectrum once (the
+// frames of a frame group share theirs), the time-domain blocks written, and
+// the Kalman state.
+double group_bytes(const Deferred& d, const Group& g) {
+  double bytes = 0.0;
+  std::vector<const void*> seen;
+  for (int r : g.recs) {
+    if (g.phase == PH_FWD) {
+      const fft3d::Geom& q = d.fwd[r].a.g;
+      bytes += (double)q.W * q.H * d.fwd[r].bytes + (double)q.nblocks * q.bh * q.nh * 8;
+    } else if (g.phase == PH_INV) {
+      const fft3d::InverseArgs& a = d.inv[r].a;
+      const double S = (double)a.g.nblocks * a.g.bh * a.g.nh * 8;
+      for (const float2* p : a.in)
+        if (p && std::find(seen.begin(), seen.end(), (const void*)p) == seen.end()) {
+          seen.push_back(p);
+          bytes += S;
+        }
+      bytes += (double)a.g.nblocks * a.g.bh * a.g.bw * 4;
+      if (d.inv[r].mode == 0) bytes += 2.0 * S * 2;
+    } else if (g.phase == PH_COPY) {
+      bytes += 2.0 * d.copies[r].width * d.copies[r].height;
+    } else {
+      const fft3d::Geom& q = d.ola[r].a.g;
+      bytes += (double)q.nblocks * q.bh * q.bw * 4 + (double)q.W * q.H * d.ola[r].bytes;
+    }
+  }
+  return bytes;
+}
+
+// Untuned steps with frame groups take their work items interleaved across
+// records, so that the resident CTAs of all frames of a group work on the
+// same blocks (and share their window spectra in L2).
+void interleave_all(Plan& plan) {
+  for (auto& g : plan.groups) g.sched.interleave = 1;
+}
+
 void set_grids(fft3d_batch* b, Plan& plan) {
   for (auto& g : plan.groups) {
     const int which = g.phase;
@@ -401,6 +449,10 @@ void fft3d_batch_destroy(fft3d_batch* b) {
   cudaSetDevice(b->device);
   cudaDeviceSynchronize();
   b->graphs.clear();
+  for (auto& p : b->pending) {
+    cudaEventDestroy(p.a);
+    cudaEventDestroy(p.b);
+  }
   if (b->direct_done) cudaEventDestroy(b->direct_done);
   if (b->h_direct) cudaFreeHost(b->h_direct);
   if (b->d_direct) cudaFree(b->d_direct);
@@ -422,11 +474,28 @@ int fft3d_batch_step(fft3d_batch* b, int count, fft3d_plane* const* planes, cons
   std::lock_guard<std::mutex> lk(b->mu);
   cudaSetDevice(b->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  // every plane stays locked until its recorded work is queued
-  std::vector<fft3d_plane*> order(planes, planes + count);
-  std::sort(order.begin(), order.end());
-  if (std::adjacent_find(order.begin(), order.end()) != order.end())
-    return fft3d::engine_fail(FFT3D_E_PARAM, "neo_fft3d: a plane appears twice in one batch step");
+  // A plane may appear several times with consecutive frames (a frame
+  // group): n, n + 1, ... in item order. Every plane stays locked until its
+  // recorded work is queued.
+  std::map<fft3d_plane*, fft3d::FrameGroup> groups;
+  for (int i = 0; i < count; i++) {
+    auto it = groups.find(planes[i]);
+    if (it == groups.end()) {
+      groups[planes[i]] = fft3d::FrameGroup{n[i], 1, 0};
+      continue;
+    }
+    fft3d::FrameGroup& g = it->second;
+    if (n[i] != g.n0 + g.count)
+      return fft3d::engine_fail(FFT3D_E_PARAM,
+                                "neo_fft3d: a plane appears twice in one batch step with frames that are not "
+                                "consecutive (n, n + 1, ...)");
+    if (planes[i] && fft3d::plane_bt(planes[i]) == 0)
+      return fft3d::engine_fail(FFT3D_E_PARAM,
+                                "neo_fft3d: a Kalman plane (bt = 0) appears twice in one batch step");
+    g.count++;
+  }
+  std::vector<fft3d_plane*> order;
+  for (auto& kv : groups) order.push_back(kv.first);
   for (auto* P : order) {
     if (!P) return fft3d::engine_fail(FFT3D_E_PARAM, "neo_fft3d: null plane in batch step");
     if (fft3d::plane_device(P) != b->device)
@@ -436,11 +505,21 @@ int fft3d_batch_step(fft3d_batch* b, int count, fft3d_plane* const* planes, cons
   }
   std::vector<std::unique_lock<std::mutex>> locks;
   for (auto* P : order) locks.emplace_back(fft3d::plane_mutex(P));
+  bool grouped = false;
+  for (auto& kv : groups) grouped = grouped || kv.second.count > 1;
   Deferred d;
+  // the frames of a group share one CTA order, alternating from step to step
+  const int reverse = (int)((uint64_t)b->stats[0] & 1);
+  for (auto& kv : groups) kv.second.reverse = reverse;
   for (int i = 0; i < count; i++) {
     d.plane = i;
-    int rc = fft3d::plane_plan(planes[i], n[i], src + 5 * i, src_stride + 5 * i, dst[i], dst_stride[i], s, &d);
-    if (rc) return rc;
+    const fft3d::FrameGroup& g = groups[planes[i]];
+    int rc = fft3d::plane_plan(planes[i], n[i], src + 5 * i, src_stride + 5 * i, dst[i], dst_stride[i], s, &d,
+                               g.count > 1 ? &g : nullptr);
+    if (rc) {
+      for (auto* P : order) fft3d::plane_discard(P, d);
+      return rc;
+    }
   }
   cudaSetDevice(b->device);
   Plan shape;  // the step's shape (one wave) keys its tuning
@@ -456,6 +535,7 @@ int fft3d_batch_step(fft3d_batch* b, int count, fft3d_plane* const* planes, cons
   if (t.stage == 0) {
     // tuning, stage 0: the wave budget, default schedules, whole step timed
     build_groups(d, count, kBudgets[t.next], plan);
+    if (grouped) interleave_all(plan);
     set_grids(b, plan);
     cudaEvent_t ev[2];
     cudaEventCreate(&ev[0]);
@@ -512,10 +592,21 @@ int fft3d_batch_step(fft3d_batch* b, int count, fft3d_plane* const* planes, cons
     }
     return FFT3D_OK;
   }
-  if (t.best.size() == plan.groups.size())
+  if (t.best.size() == plan.groups.size()) {
     for (size_t gi = 0; gi < plan.groups.size(); gi++) plan.groups[gi].sched = t.best[gi];
+  } else if (grouped) {
+    interleave_all(plan);
+  }
   set_grids(b, plan);
   b->stats[6] = (double)(t.budget >> 20);
+  if (b->timing) {
+    std::vector<cudaEvent_t> ev(2 * plan.groups.size());
+    for (auto& e : ev) CK(cudaEventCreate(&e), "batch timing event");
+    int rc = run_direct(b, plan, d, s, &ev);
+    for (size_t gi = 0; gi < plan.groups.size(); gi++)
+      b->pending.push_back({plan.groups[gi].phase, group_bytes(d, plan.groups[gi]), ev[2 * gi], ev[2 * gi + 1]});
+    return rc;
+  }
   auto& slot = b->graphs[plan.sig];
   if (!slot) {
     slot.reset(new Captured);
@@ -536,6 +627,35 @@ int fft3d_batch_step(fft3d_batch* b, int count, fft3d_plane* const* planes, cons
   c->parity ^= 1;
   b->stats[1] += 1;
   return FFT3D_OK;
+}
+
+int fft3d_batch_set_timing(fft3d_batch* b, int enable) {
+  if (!b) return fft3d::engine_fail(FFT3D_E_PARAM, "neo_fft3d: null handle");
+  std::lock_guard<std::mutex> lk(b->mu);
+  b->timing = enable != 0;
+  return FFT3D_OK;
+}
+
+int fft3d_batch_timing(fft3d_batch* b, double out[12]) {
+  if (!b || !out) return fft3d::engine_fail(FFT3D_E_PARAM, "neo_fft3d: null argument");
+  std::lock_guard<std::mutex> lk(b->mu);
+  cudaSetDevice(b->device);
+  int rc = FFT3D_OK;
+  for (auto& p : b->pending) {
+    float ms = 0.f;
+    cudaError_t e = cudaEventSynchronize(p.b);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, p.a, p.b);
+    if (e != cudaSuccess && rc == FFT3D_OK) rc = cuda_fail(e, "batch timing");
+    b->t_phase[p.phase][0] += 1;
+    b->t_phase[p.phase][1] += ms;
+    b->t_phase[p.phase][2] += p.bytes;
+    cudaEventDestroy(p.a);
+    cudaEventDestroy(p.b);
+  }
+  b->pending.clear();
+  for (int ph = 0; ph < 4; ph++)
+    for (int k = 0; k < 3; k++) out[3 * ph + k] = b->t_phase[ph][k];
+  return rc;
 }
 
 int fft3d_batch_stats(fft3d_batch* b, double out[8]) {

@@ -26,12 +26,25 @@ struct Deferred {
   std::vector<Copy> copies;  // device-to-device, before the overlap-add phase
 };
 
+// Consecutive output frames n0 .. n0 + count - 1 of one plane planned into
+// one step (Wiener/sharpen planes only: Kalman state runs frame to frame).
+struct FrameGroup {
+  int n0, count;
+  int reverse;  // CTA order shared by the group's frames
+};
+
 // Runs plane P's per-frame control for output frame n (device buffers) with
 // every launch and copy recorded in d; the spectrum-ring bookkeeping is done
-// as if they had been issued. The caller holds plane_mutex(P) until the
-// recorded work is queued.
+// as if they had been issued. With a frame group, n is one of its frames:
+// its time-domain buffer is the group's k-th, and every spectrum the group
+// needs stays in the ring (grown as needed). The caller holds
+// plane_mutex(P) until the recorded work is queued.
 int plane_plan(fft3d_plane* P, int n, const void* const src[5], const int stride[5], void* dst, int dst_stride,
-               cudaStream_t st, Deferred* d);
+               cudaStream_t st, Deferred* d, const FrameGroup* grp = nullptr);
+int plane_bt(const fft3d_plane* P);
+// Forgets the spectra whose forward transforms d recorded for P (planning
+// failed, so they will not run).
+void plane_discard(fft3d_plane* P, const Deferred& d);
 std::mutex& plane_mutex(fft3d_plane* P);
 int plane_device(const fft3d_plane* P);
 // Empty when the scheduler can take the plane, else the reason.

@@ -86,6 +86,15 @@ struct fft3d_plane {
   std::vector<Slot> slots;
   uint64_t clock = 0;
   float* d_tdom = nullptr;
+  // Frame groups (several consecutive output frames of this plane in one
+  // batch step): occurrence k > 0 of the group writes its time-domain blocks
+  // to tdom_extra[k - 1]; frames in [keep_lo, keep_hi] stay in the ring while
+  // the group is planned; all frames of a group use one CTA order.
+  std::vector<float*> tdom_extra;
+  int occ = 0;
+  int keep_lo = 1, keep_hi = 0;
+  int fixed_reverse = -1;
+  uint64_t groups_done = 0;  // frame groups filtered (their CTA order alternates)
   float2* d_last = nullptr;
   float* d_cov = nullptr;
   float* d_covp = nullptr;
@@ -270,6 +279,7 @@ void free_plane(fft3d_plane* P) {
   for (auto& s : P->slots) cudaFree(s.spec);
   cudaFree(P->d_tables);
   cudaFree(P->d_tdom);
+  for (auto* t : P->tdom_extra) cudaFree(t);
   cudaFree(P->d_filt);
   cudaFree(P->d_tc);
   cudaFree(P->d_err);
@@ -307,11 +317,14 @@ Slot* find_slot(fft3d_plane* P, int frame) {
   return nullptr;
 }
 
-// least recently used slot whose frame is not in [lo, hi]
+// least recently used slot whose frame is not in [lo, hi] (nor in the
+// frame group's kept range); free slots (frame -1) are always candidates
 Slot* evict_slot(fft3d_plane* P, int lo, int hi) {
   Slot* best = nullptr;
   for (auto& s : P->slots) {
-    if (s.frame >= lo && s.frame <= hi) continue;
+    const bool free_slot = s.frame < 0;  // frames are >= 0
+    if (!free_slot && s.frame >= lo && s.frame <= hi) continue;
+    if (!free_slot && s.frame >= P->keep_lo && s.frame <= P->keep_hi) continue;
     if (!best || s.stamp < best->stamp) best = &s;
   }
   return best;
@@ -517,10 +530,12 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
   ia.kal_last = P->d_last;
   ia.kal_covar = P->d_cov;
   ia.kal_covarp = P->d_covp;
-  ia.tdom = P->d_tdom;
+  float* tdom = P->occ > 0 ? P->tdom_extra[P->occ - 1] : P->d_tdom;
+  ia.tdom = tdom;
   ia.err = P->d_err;
   ia.bulk = (P->path == 1 || P->path == 3) ? P->bulk : 0;
   ia.reverse = (int)(P->frames_done++ & 1);
+  if (P->fixed_reverse >= 0) ia.reverse = P->fixed_reverse;
   {
     const double S = (double)P->spec_elems() * sizeof(float2);
     const double state = bt == 0 ? 2.0 * (double)P->spec_elems() * 16 : 0.0;
@@ -585,7 +600,7 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
   fft3d::OlaArgs oa;
   oa.g = P->g;
   oa.t = P->tab;
-  oa.tdom = P->d_tdom;
+  oa.tdom = tdom;
   oa.dst = static_cast<char*>(odst) + (long long)P->t * ostride + (long long)P->l * P->bytes;
   oa.dst_stride = ostride;
   oa.norm = P->norm;
@@ -623,6 +638,93 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
 }
 
 // Waits for a queued host-path call and reports a device error flag it saw.
+// Frames whose spectra a frame group n0 .. n0 + count - 1 needs at once.
+void group_range(const fft3d_plane* P, int n0, int count, int* lo, int* hi) {
+  const int bt = std::max(P->ep.bt, 1);
+  *lo = n0 - bt / 2;
+  *hi = n0 + count - 1 + (bt - 1) / 2;
+}
+
+// A frame group keeps the spectra of frames lo..hi in the ring at once and
+// writes one time-domain buffer per frame: both grow on first use.
+int group_resources(fft3d_plane* P, int lo, int hi, int count) {
+  while ((int)P->slots.size() < hi - lo + 2) {
+    Slot s;
+    if (cudaMalloc(&s.spec, P->spec_elems() * sizeof(float2)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (spectrum ring of a frame group)");
+    }
+    P->slots.push_back(s);
+  }
+  while ((int)P->tdom_extra.size() < count - 1) {
+    float* t = nullptr;
+    if (cudaMalloc(&t, (size_t)P->g.nblocks * P->g.bh * P->g.bw * sizeof(float)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (time-domain blocks of a frame group)");
+    }
+    P->tdom_extra.push_back(t);
+  }
+  return FFT3D_OK;
+}
+
+// Recorded forward transforms that will not run (planning failed): their
+// slots hold no spectrum.
+void discard_recorded(fft3d_plane* P, const fft3d::Deferred& d) {
+  for (const auto& f : d.fwd)
+    for (auto& s : P->slots)
+      if (s.spec == f.a.spec) s.frame = -1;
+}
+
+// Issues the launches of a frame group recorded for plane P, phase by phase:
+// the new spectra, then the filter/inverse of runs of consecutive frames of
+// one Wiener 3D mode as one k_filter_inverse_frames launch each (the other
+// frames, e.g. the clip-edge ones, one launch each), the crop-border copies
+// and the overlap-adds.
+int run_group(fft3d_plane* P, const fft3d::Deferred& d, cudaStream_t st) {
+  const double S = (double)P->spec_elems() * sizeof(float2);
+  const double T = (double)P->g.nblocks * P->g.bh * P->g.bw * 4;
+  const double pix = (double)P->g.W * P->g.H * P->bytes;
+  for (const auto& f : d.fwd) {
+    TimeScope ts(P, K_FORWARD, pix + S, st);
+    CK(fft3d::launch_forward(f.a, f.bytes, st), "forward kernel");
+    g_launches++;
+  }
+  for (size_t i = 0; i < d.inv.size();) {
+    const int mode = d.inv[i].mode;
+    size_t e = i + 1;
+    if (mode >= 2)
+      while (e < d.inv.size() && d.inv[e].mode == mode && (int)(e - i) < fft3d::kMaxGroupFrames) e++;
+    std::vector<const float2*> seen;
+    for (size_t k = i; k < e; k++)
+      for (const float2* p : d.inv[k].a.in)
+        if (p && std::find(seen.begin(), seen.end(), p) == seen.end()) seen.push_back(p);
+    // reads: each window spectrum of the run once; writes: the time-domain blocks
+    TimeScope ts(P, K_INVERSE, (double)seen.size() * S + (double)(e - i) * T, st);
+    if (e - i == 1) {
+      CK(fft3d::launch_filter_inverse(d.inv[i].a, mode, st), "filter/inverse kernel");
+    } else {
+      fft3d::FrameSet fs{};
+      fs.count = (int)(e - i);
+      for (size_t k = i; k < e; k++) {
+        for (int w = 0; w < 5; w++) fs.in[k - i][w] = d.inv[k].a.in[w];
+        fs.tdom[k - i] = d.inv[k].a.tdom;
+      }
+      CK(fft3d::launch_filter_inverse_frames(d.inv[i].a, fs, mode, st), "filter/inverse kernel (frame group)");
+    }
+    g_launches++;
+    i = e;
+  }
+  for (const auto& c : d.copies)
+    CK(cudaMemcpy2DAsync(c.dst, c.dpitch, c.src, c.spitch, c.width, c.height, cudaMemcpyDeviceToDevice, st),
+       "plane copy");
+  for (const auto& o : d.ola) {
+    TimeScope ts(P, K_OLA, T + pix, st);
+    CK(fft3d::launch_overlap_add(o.a, o.bytes, st), "overlap-add kernel");
+    g_launches++;
+  }
+  return FFT3D_OK;
+}
+
 int finish_call(fft3d_plane* P, cudaEvent_t done, fft3d_plane::Stage* sg, bool learned) {
   const cudaError_t e = cudaEventSynchronize(done);
   give_sync_event(P, done);
@@ -645,13 +747,30 @@ namespace fft3d {
 void set_last_error(const std::string& msg) { g_err = msg; }
 
 int plane_plan(fft3d_plane* P, int n, const void* const src[5], const int stride[5], void* dst, int dst_stride,
-               cudaStream_t st, Deferred* d) {
+               cudaStream_t st, Deferred* d, const FrameGroup* grp) {
   cudaSetDevice(P->device);
+  if (grp) {
+    int lo, hi;
+    group_range(P, grp->n0, grp->count, &lo, &hi);
+    int rc = group_resources(P, lo, hi, grp->count);
+    if (rc) return rc;
+    P->occ = n - grp->n0;
+    P->keep_lo = lo;
+    P->keep_hi = hi;
+    P->fixed_reverse = grp->reverse;
+  }
   g_defer = d;
   const int rc = run_filter(P, n, src, stride, dst, dst_stride, false, st);
   g_defer = nullptr;
+  P->occ = 0;
+  P->keep_lo = 1;
+  P->keep_hi = 0;
+  P->fixed_reverse = -1;
   return rc;
 }
+
+int plane_bt(const fft3d_plane* P) { return P->ep.bt; }
+void plane_discard(fft3d_plane* P, const Deferred& d) { discard_recorded(P, d); }
 
 std::mutex& plane_mutex(fft3d_plane* P) { return P->mu; }
 int plane_device(const fft3d_plane* P) { return P->device; }
@@ -945,6 +1064,49 @@ int fft3d_plane_filter_device(fft3d_plane* P, int n, const void* const src[5], c
   std::lock_guard<std::mutex> lk(P->mu);
   CK(cudaSetDevice(P->device), "cudaSetDevice");
   return run_filter(P, n, src, src_stride, dst, dst_stride, false, stream ? (cudaStream_t)stream : P->stream);
+}
+
+int fft3d_plane_filter_frames_device(fft3d_plane* P, int n0, int count, const void* const* src, const int* src_stride,
+                                     void* const* dst, const int* dst_stride, void* stream) {
+  if (!P || !src || !src_stride || !dst || !dst_stride || count < 1 || count > FFT3D_MAX_FRAME_GROUP)
+    return fail(FFT3D_E_PARAM, "neo_fft3d: invalid frame group arguments");
+  for (int j = 0; j < count; j++)
+    if (!dst[j]) return fail(FFT3D_E_PARAM, "neo_fft3d: null output frame in a frame group");
+  std::lock_guard<std::mutex> lk(P->mu);
+  CK(cudaSetDevice(P->device), "cudaSetDevice");
+  cudaStream_t st = stream ? (cudaStream_t)stream : P->stream;
+  // frame n0 + j reads the window src[j .. j + 4]
+  if (count == 1 || P->ep.bt < 2 || !fft3d::plane_batchable(P).empty()) {
+    for (int j = 0; j < count; j++) {
+      int rc = run_filter(P, n0 + j, src + j, src_stride + j, dst[j], dst_stride[j], false, st);
+      if (rc) return rc;
+    }
+    return FFT3D_OK;
+  }
+  int lo, hi;
+  group_range(P, n0, count, &lo, &hi);
+  int rc = group_resources(P, lo, hi, count);
+  if (rc) return rc;
+  fft3d::Deferred d;
+  P->keep_lo = lo;
+  P->keep_hi = hi;
+  P->fixed_reverse = (int)(P->groups_done++ & 1);
+  for (int j = 0; j < count && rc == FFT3D_OK; j++) {
+    P->occ = j;
+    d.plane = j;
+    g_defer = &d;
+    rc = run_filter(P, n0 + j, src + j, src_stride + j, dst[j], dst_stride[j], false, st);
+    g_defer = nullptr;
+  }
+  P->occ = 0;
+  P->keep_lo = 1;
+  P->keep_hi = 0;
+  P->fixed_reverse = -1;
+  if (rc) {
+    discard_recorded(P, d);
+    return rc;
+  }
+  return run_group(P, d, st);
 }
 
 int fft3d_plane_cached(fft3d_plane* P, int n) {

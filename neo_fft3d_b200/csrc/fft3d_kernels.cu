@@ -153,6 +153,11 @@ cudaError_t launch_filter_inverse(const InverseArgs& a, int mode, cudaStream_t s
   return e ? e->inv(a, mode, s) : cudaErrorInvalidValue;
 }
 
+cudaError_t launch_filter_inverse_frames(const InverseArgs& a, const FrameSet& fs, int mode, cudaStream_t s) {
+  const SizeEntry* e = find_size(a.g.bw, a.g.bh);
+  return e ? e->inv_frames(a, fs, mode, s) : cudaErrorInvalidValue;
+}
+
 cudaError_t launch_filter_bins(const InverseArgs& a, float2* F, int mode, cudaStream_t s) {
   const int bins = a.g.bh * a.g.nh;
   const size_t pairs = (size_t)a.g.nblocks * bins / 2;

@@ -93,6 +93,16 @@ struct InverseArgs {
                           // that the blocks read last stay in L2 for the next frame)
 };
 
+// The per-frame part of a frame group's filter/inverse launch: frame j's
+// window spectra (slots n-2..n+2 of its InverseArgs::in) and time-domain
+// buffer.
+constexpr int kMaxGroupFrames = 16;
+struct FrameSet {
+  const float2* in[kMaxGroupFrames][5];
+  float* tdom[kMaxGroupFrames];
+  int count;
+};
+
 // Forward transform of the window's newest frame fused with the filter and
 // the inverse transform (k_fused). f.src/f.spec: the newest frame and its ring
 // slot; v.in[]: the window's spectra (the newest frame's entry is f.spec).
@@ -135,6 +145,9 @@ struct CopyArgs {
 // Host-side launchers (fft3d_kernels.cu). They return cudaGetLastError().
 cudaError_t launch_forward(const ForwardArgs& a, int bytes_per_sample, cudaStream_t s);
 cudaError_t launch_filter_inverse(const InverseArgs& a, int mode, cudaStream_t s);
+// Frame group: fs.count consecutive output frames of one plane (Wiener 3D,
+// mode 2..5) in one launch; a holds everything they share.
+cudaError_t launch_filter_inverse_frames(const InverseArgs& a, const FrameSet& fs, int mode, cudaStream_t s);
 cudaError_t launch_overlap_add(const OlaArgs& a, int bytes_per_sample, cudaStream_t s);
 // Batched forms (work items as in BatchLaunch); OLA items are 32x8-pixel tiles.
 cudaError_t launch_forward_batch(int bw, int bh, const BatchLaunch& l, int bytes_per_sample, cudaStream_t s);

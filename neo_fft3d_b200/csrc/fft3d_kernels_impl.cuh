@@ -484,10 +484,25 @@ __host__ __device__ constexpr int fft_ctas(int nblocks) {
   return (nblocks + kWarps * blocks_per_warp<BW>() - 1) / (kWarps * blocks_per_warp<BW>());
 }
 
+// Where a CTA finds its window spectra and writes its time-domain blocks:
+// the launch arguments (one output frame per launch), or pointers picked for
+// one frame of a frame group (k_filter_inverse_frames).
+struct ArgsWin {
+  const InverseArgs& a;
+  __device__ __forceinline__ const float2* in(int k) const { return a.in[k]; }
+  __device__ __forceinline__ float* tdom() const { return a.tdom; }
+};
+struct FrameWin {
+  const float2* p[5];
+  float* t;
+  __device__ __forceinline__ const float2* in(int k) const { return p[k]; }
+  __device__ __forceinline__ float* tdom() const { return t; }
+};
+
 // NEWEST_IN_S: the window's newest frame (slot win_hi) is not read from
-// a.in[] but from S, where the fused kernel's forward transform left it.
-template <int BW, int BH, int MODE, bool NEWEST_IN_S = false>
-__device__ __forceinline__ void filter_inverse_cta(const InverseArgs& a, int vcta) {
+// the window but from S, where the fused kernel's forward transform left it.
+template <int BW, int BH, int MODE, bool NEWEST_IN_S, class Win>
+__device__ __forceinline__ void filter_inverse_cta_w(const InverseArgs& a, int vcta, const Win& win) {
   constexpr int NH = BW / 2 + 1, HC = BW / 2, NBW = blocks_per_warp<BW>(), BINS = BH * NH;
   constexpr int PER = (BINS + 31) / 32;
   extern __shared__ float2 smem2[];
@@ -516,7 +531,7 @@ __device__ __forceinline__ void filter_inverse_cta(const InverseArgs& a, int vct
         gf = a.c.degrid * S[b * BINS].x / gs0;
         __syncwarp();  // every lane has the DC before lane 0 overwrites it
       } else {
-        gf = a.c.degrid * __ldg(&a.in[2][off].x) / gs0;
+        gf = a.c.degrid * __ldg(&win.in(2)[off].x) / gs0;
       }
     }
     // software pipeline: the window's values of chunk j + D are loaded while
@@ -525,7 +540,7 @@ __device__ __forceinline__ void filter_inverse_cta(const InverseArgs& a, int vct
     auto load = [&](int j, float2(&dst)[NGB]) {
       const int i = lane + 32 * j;
 #pragma unroll
-      for (int k = 0; k < NG; k++) dst[k] = i < BINS ? __ldg(a.in[LO + k] + off + i) : make_float2(0.f, 0.f);
+      for (int k = 0; k < NG; k++) dst[k] = i < BINS ? __ldg(win.in(LO + k) + off + i) : make_float2(0.f, 0.f);
     };
     if constexpr (NG > 0) {
 #pragma unroll
@@ -562,8 +577,38 @@ __device__ __forceinline__ void filter_inverse_cta(const InverseArgs& a, int vct
   }
   __syncwarp();
   for (int b = 0; b < NBW && blk0 + b < g.nblocks; b++)
-    store_tdom<BW, BH>(S + b * BINS, a.tdom + (size_t)(blk0 + b) * BH * BW, lane);
+    store_tdom<BW, BH>(S + b * BINS, win.tdom() + (size_t)(blk0 + b) * BH * BW, lane);
   __syncwarp();  // S is reused by the warp's next work item
+}
+
+template <int BW, int BH, int MODE, bool NEWEST_IN_S = false>
+__device__ __forceinline__ void filter_inverse_cta(const InverseArgs& a, int vcta) {
+  filter_inverse_cta_w<BW, BH, MODE, NEWEST_IN_S, ArgsWin>(a, vcta, ArgsWin{a});
+}
+
+// Several consecutive output frames of one plane in one launch (a frame
+// group). CTA x works on frame x % count, CTA-of-frame x / count: the
+// resident CTAs of all the group's frames cover the same blocks at the same
+// time, so a window spectrum shared by up to bt frames is read from HBM once
+// and then hit in L2. The frames differ only in their window spectra and
+// time-domain buffers (fs); everything else is in a.
+template <int BW, int BH, int MODE>
+__global__ void __launch_bounds__(kWarps * 32) k_filter_inverse_frames(InverseArgs a, FrameSet fs) {
+  const int j = blockIdx.x % fs.count, c = blockIdx.x / fs.count;
+  // the frame's pointers, selected with constant indices (a dynamic index
+  // into the parameter space would copy it to local memory)
+  FrameWin w;
+#pragma unroll
+  for (int k = 0; k < 5; k++) w.p[k] = nullptr;
+  w.t = nullptr;
+#pragma unroll
+  for (int q = 0; q < kMaxGroupFrames; q++)
+    if (q == j) {
+#pragma unroll
+      for (int k = 0; k < 5; k++) w.p[k] = fs.in[q][k];
+      w.t = fs.tdom[q];
+    }
+  filter_inverse_cta_w<BW, BH, MODE, false, FrameWin>(a, c, w);
 }
 
 template <int BW, int BH, int MODE>
@@ -870,6 +915,29 @@ cudaError_t fused_sized(const FusedArgs& a, int mode, int bytes, cudaStream_t s)
   return cudaErrorNotSupported;  // float samples use the unfused path
 }
 
+template <int BW, int BH, int MODE>
+cudaError_t inv_frames_mode(const InverseArgs& a, const FrameSet& fs, cudaStream_t s) {
+  const int smem = kWarps * fft_smem_bytes<BW, BH>();
+  const int grid = fft_grid<BW, BH>(a.g.nblocks) * fs.count;
+  cudaError_t e = fft3d::smem_attr(k_filter_inverse_frames<BW, BH, MODE>, smem);
+  if (e != cudaSuccess) return e;
+  k_filter_inverse_frames<BW, BH, MODE><<<grid, kWarps * 32, smem, s>>>(a, fs);
+  return cudaGetLastError();
+}
+
+// frame groups: Wiener 3D windows (the modes whose frames share spectra)
+template <int BW, int BH>
+cudaError_t inv_frames(const InverseArgs& a, const FrameSet& fs, int mode, cudaStream_t s) {
+  if (fs.count < 1 || fs.count > kMaxGroupFrames) return cudaErrorInvalidValue;
+  switch (mode) {
+    case 2: return inv_frames_mode<BW, BH, 2>(a, fs, s);
+    case 3: return inv_frames_mode<BW, BH, 3>(a, fs, s);
+    case 4: return inv_frames_mode<BW, BH, 4>(a, fs, s);
+    case 5: return inv_frames_mode<BW, BH, 5>(a, fs, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
 template <int BW, int BH>
 cudaError_t inv_sized(const InverseArgs& a, int mode, cudaStream_t s) {
   switch (mode) {
@@ -890,6 +958,7 @@ cudaError_t inv_sized(const InverseArgs& a, int mode, cudaStream_t s) {
 #define FFT3D_REGISTER_SIZE(BW, BH)                                                                     \
   static const bool fft3d_reg_##BW##x##BH = register_size(                                             \
       SizeEntry{BW, BH, &fwd_sized<BW, BH>, &inv_sized<BW, BH>, &fused_sized<BW, BH>, &upload_twiddle_table, \
-                &fwd_batch<BW, BH>, &inv_batch<BW, BH>, &ctas_per_plane<BW, BH>, &occupancy_of<BW, BH>});
+                &fwd_batch<BW, BH>, &inv_batch<BW, BH>, &ctas_per_plane<BW, BH>, &occupancy_of<BW, BH>,      \
+                &inv_frames<BW, BH>});
 
 }  // namespace fft3d

@@ -19,6 +19,8 @@ struct SizeEntry {
   cudaError_t (*inv_batch)(const BatchLaunch&, int mode, cudaStream_t);
   int (*ctas)(int nblocks);                       // work items (CTAs) per plane
   int (*occupancy)(int which, int mode_or_bytes);  // resident CTAs per SM: 0 forward, 1 filter/inverse
+  // frame groups (Wiener 3D modes 2..5): several output frames in one launch
+  cudaError_t (*inv_frames)(const InverseArgs&, const FrameSet&, int mode, cudaStream_t);
 };
 
 bool register_size(const SizeEntry& e);

@@ -41,6 +41,8 @@ def lib():
                                          ctypes.POINTER(vp)]
         L.fft3d_plane_filter.argtypes = [vp, ci, ctypes.POINTER(vp), ctypes.POINTER(ci), vp, ci]
         L.fft3d_plane_filter_device.argtypes = [vp, ci, ctypes.POINTER(vp), ctypes.POINTER(ci), vp, ci, vp]
+        L.fft3d_plane_filter_frames_device.argtypes = [vp, ci, ci, ctypes.POINTER(vp), ctypes.POINTER(ci),
+                                                       ctypes.POINTER(vp), ctypes.POINTER(ci), vp]
         L.fft3d_plane_cached.argtypes = [vp, ci]
         L.fft3d_plane_spectrum.argtypes = [vp, ci, vp]
         L.fft3d_plane_geometry.argtypes = [vp, ctypes.POINTER(ci)]
@@ -58,6 +60,8 @@ def lib():
         L.fft3d_batch_step.argtypes = [vp, ci, ctypes.POINTER(vp), ctypes.POINTER(ci), ctypes.POINTER(vp),
                                        ctypes.POINTER(ci), ctypes.POINTER(vp), ctypes.POINTER(ci), vp]
         L.fft3d_batch_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+        L.fft3d_batch_set_timing.argtypes = [vp, ci]
+        L.fft3d_batch_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         _lib = L
     return _lib
 
@@ -104,6 +108,20 @@ class PlaneEngine:
         s = (ctypes.c_int * 5)(*strides)
         _check(lib().fft3d_plane_filter_device(self.h, n, p, s, ctypes.c_void_p(dst_ptr), dst_stride,
                                                ctypes.c_void_p(stream) if stream else None))
+
+    def filter_frames_device(self, n0: int, ptrs, strides, dst_ptrs, dst_strides, stream: int = 0):
+        """Filter frames n0 .. n0 + len(dst_ptrs) - 1 in one call (a frame
+        group): ptrs[j] / strides[j] are frame n0 - 2 + j (len(dst_ptrs) + 4
+        entries, 0 outside the clip); queued on `stream`."""
+        count = len(dst_ptrs)
+        if len(ptrs) != count + 4 or len(strides) != count + 4 or len(dst_strides) != count:
+            raise ValueError("filter_frames_device: ptrs/strides need count + 4 entries, dst_strides count")
+        p = (ctypes.c_void_p * (count + 4))(*[x or None for x in ptrs])
+        s = (ctypes.c_int * (count + 4))(*strides)
+        d = (ctypes.c_void_p * count)(*dst_ptrs)
+        ds = (ctypes.c_int * count)(*dst_strides)
+        _check(lib().fft3d_plane_filter_frames_device(self.h, n0, count, p, s, d, ds,
+                                                      ctypes.c_void_p(stream) if stream else None))
 
     def cached(self, n: int) -> bool:
         return bool(lib().fft3d_plane_cached(self.h, n))
@@ -159,17 +177,38 @@ class Batch:
         self.h = h
         _check(lib().fft3d_batch_set_tuning(self.h, 1 if tuning else 0))
 
-    def step(self, items, stream: int = 0):
-        """items: list of (PlaneEngine, n, src_ptrs[5], src_strides[5], dst_ptr, dst_stride)."""
+    class Prepared(tuple):
+        """C arrays of a step's items (Batch.prepare)."""
+
+    @staticmethod
+    def prepare(items):
+        """The C arrays of a step's items, for repeated steps over fixed buffers."""
         k = len(items)
-        planes = (ctypes.c_void_p * k)(*[it[0].h.value for it in items])
-        ns = (ctypes.c_int * k)(*[it[1] for it in items])
-        src = (ctypes.c_void_p * (5 * k))(*[p or None for it in items for p in it[2]])
-        sst = (ctypes.c_int * (5 * k))(*[x for it in items for x in it[3]])
-        dst = (ctypes.c_void_p * k)(*[it[4] for it in items])
-        dstr = (ctypes.c_int * k)(*[it[5] for it in items])
+        return Batch.Prepared((k, (ctypes.c_void_p * k)(*[it[0].h.value for it in items]),
+                               (ctypes.c_int * k)(*[it[1] for it in items]),
+                               (ctypes.c_void_p * (5 * k))(*[p or None for it in items for p in it[2]]),
+                               (ctypes.c_int * (5 * k))(*[x for it in items for x in it[3]]),
+                               (ctypes.c_void_p * k)(*[it[4] for it in items]),
+                               (ctypes.c_int * k)(*[it[5] for it in items])))
+
+    def step(self, items, stream: int = 0):
+        """items: list of (PlaneEngine, n, src_ptrs[5], src_strides[5], dst_ptr, dst_stride),
+        or the result of prepare(items). A plane may appear with consecutive
+        frames n, n + 1, ... (a frame group; not for Kalman planes)."""
+        k, planes, ns, src, sst, dst, dstr = items if isinstance(items, Batch.Prepared) else self.prepare(items)
         _check(lib().fft3d_batch_step(self.h, k, planes, ns, src, sst, dst, dstr,
                                       ctypes.c_void_p(stream) if stream else None))
+
+    def set_timing(self, enable: bool = True):
+        """Per-phase kernel timing of tuned steps (they then run without their graph)."""
+        _check(lib().fft3d_batch_set_timing(self.h, 1 if enable else 0))
+
+    def timing(self) -> dict:
+        """{phase: (launches, ms, algorithmic bytes)} since creation (waits for the timed launches)."""
+        out = (ctypes.c_double * 12)()
+        _check(lib().fft3d_batch_timing(self.h, out))
+        names = ("forward", "filter_inverse", "copy", "overlap_add")
+        return {k: (int(out[3 * i]), out[3 * i + 1], out[3 * i + 2]) for i, k in enumerate(names)}
 
     def stats(self) -> dict:
         out = (ctypes.c_double * 8)()

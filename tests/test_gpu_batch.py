@@ -118,3 +118,105 @@ def test_batch_rejects_bad_steps(gpu, monkeypatch):
     etc.close()
     e.close()
     b.close()
+
+
+def _grouped(torch, clips, k, tuning):
+    """Steps of k consecutive frames of every Wiener/sharpen plane (a frame
+    group per plane); the last step takes what is left."""
+    engs, outs, srcs = [], [], []
+    for c in clips:
+        if c["params"].bt == 0:
+            continue
+        for a, d in zip(c["planes"], c["descs"]):
+            engs.append(engine.PlaneEngine(c["params"], d))
+            outs.append(torch.empty_like(a))
+            srcs.append(a)
+    b = engine.Batch(tuning=tuning)
+    stream = torch.cuda.current_stream().cuda_stream
+    for n0 in range(0, F, k):
+        items = []
+        for e, a, o in zip(engs, srcs, outs):
+            fb = a.shape[1] * a.shape[2] * a.element_size()
+            for n in range(n0, min(n0 + k, F)):
+                ptrs, st = _window(a, n, F)
+                items.append((e, n, ptrs, st, o.data_ptr() + n * fb, a.shape[2] * a.element_size()))
+        b.step(items, stream)
+    torch.cuda.synchronize()
+    stats = b.stats()
+    b.close()
+    for e in engs:
+        e.close()
+    return [o.cpu().numpy() for o in outs], stats
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k,tuning", [(4, False), (3, True), (8, False)], ids=["k4", "k3_autotuned", "k8"])
+def test_frame_groups_match_per_plane(gpu, k, tuning):
+    """Several consecutive frames of each plane in one step (frame groups,
+    including the clip-edge frames with btcur = 1 and a short last group):
+    byte-identical to one-frame-at-a-time filtering."""
+    import torch
+    clips = _setup(torch)
+    ref = _per_plane(torch, [c for c in clips if c["params"].bt != 0])
+    got, stats = _grouped(torch, clips, k, tuning)
+    for i, (r, g) in enumerate(zip(ref, got)):
+        assert np.array_equal(r, g), i
+    assert stats["steps"] == (F + k - 1) // k
+
+
+@pytest.mark.gpu
+def test_frame_group_rules(gpu):
+    import torch
+    a = torch.zeros((6, 64, 64), dtype=torch.uint8, device="cuda")
+    d = plane_descs([(64, 64)], 8, 6)[0]
+    b = engine.Batch()
+    ew = engine.PlaneEngine(make_params(sigma=2.0, bt=3, bw=32, bh=32, ow=16, oh=16), d)
+    ek = engine.PlaneEngine(make_params(sigma=2.0, bt=0, bw=32, bh=32, ow=16, oh=16), d)
+
+    def item(e, n):
+        ptrs, st = _window(a, n, 6)
+        return (e, n, ptrs, st, a.data_ptr(), 64)
+
+    with pytest.raises(engine.FFT3DError, match="not consecutive"):
+        b.step([item(ew, 1), item(ew, 3)])
+    with pytest.raises(engine.FFT3DError, match="not consecutive"):
+        b.step([item(ew, 2), item(ew, 1)])
+    with pytest.raises(engine.FFT3DError, match="Kalman"):
+        b.step([item(ek, 1), item(ek, 2)])
+    ew.close()
+    ek.close()
+    b.close()
+
+
+@pytest.mark.gpu
+def test_batch_timing_counts_phases(gpu):
+    """Per-phase timing: every timed step's launches are counted, with their
+    algorithmic bytes (a frame group reads each window spectrum once)."""
+    import torch
+    clips = _setup(torch)[:1]
+    c = clips[0]
+    engs = [engine.PlaneEngine(c["params"], d) for d in c["descs"]]
+    outs = [torch.empty_like(a) for a in c["planes"]]
+    b = engine.Batch(tuning=False)
+    b.set_timing(True)
+    stream = torch.cuda.current_stream().cuda_stream
+    k = 4
+    for n0 in range(4, 12, k):
+        items = []
+        for e, a, o in zip(engs, c["planes"], outs):
+            fb = a.shape[1] * a.shape[2] * a.element_size()
+            for n in range(n0, n0 + k):
+                ptrs, st = _window(a, n, F)
+                items.append((e, n, ptrs, st, o.data_ptr() + n * fb, a.shape[2] * a.element_size()))
+        b.step(items, stream)
+    t = b.timing()
+    assert t["forward"][0] >= 1 and t["filter_inverse"][0] == 2 and t["overlap_add"][0] == 2
+    assert all(v[1] > 0 for k_, v in t.items() if v[0] > 0)
+    # filter/inverse of the second step (frames 8..11, bt = 5): spectra of
+    # frames 6..13 once per plane, and four time-domain buffers per plane
+    S = sum(e.nblocks * 32 * 17 * 8 for e in engs)
+    T = sum(e.nblocks * 32 * 32 * 4 for e in engs)
+    assert t["filter_inverse"][2] == pytest.approx(2 * (8 * S + 4 * T))
+    b.close()
+    for e in engs:
+        e.close()

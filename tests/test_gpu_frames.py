@@ -1,0 +1,152 @@
+"""Frame groups (fft3d_plane_filter_frames_device): several consecutive
+output frames of one plane in one call must give byte-identical output to
+filtering the frames one at a time (fft3d_plane_filter_device), for every
+Wiener 3D window length, block size, crop, pattern and sample type, across
+the clip-edge frames (btcur = 1) and with groups of every size; planes that
+are not grouped (Kalman, Wiener 2D, sharpen only, the tensor-core path) must
+give their per-frame output too."""
+import numpy as np
+import pytest
+
+from neo_fft3d_b200 import engine, synth
+from neo_fft3d_b200.params import make_params, plane_descs
+
+F = 23
+
+CASES = [
+    ("bt5_sharpen", dict(width=200, height=136, bits=8, seed=71), dict(sigma=3.0, bt=5, sharpen=0.3)),
+    ("bt4_bw48", dict(width=176, height=144, bits=8, seed=72), dict(sigma=2.5, bt=4, bw=48, bh=48, ow=16, oh=16)),
+    ("bt3_crop_dehalo", dict(width=160, height=128, bits=8, seed=73),
+     dict(sigma=2.0, bt=3, l=6, t=4, r=8, b=2, dehalo=0.5)),
+    ("bt2_degrid0", dict(width=144, height=112, bits=8, seed=74), dict(sigma=2.0, bt=2, degrid=0.0)),
+    ("bt5_10bit", dict(width=160, height=120, bits=10, seed=75), dict(sigma=8.0, bt=5)),
+    ("bt3_pattern", dict(width=160, height=128, bits=8, seed=76), dict(sigma=2.0, bt=3, pfactor=1.0, pframe=3)),
+    ("kalman", dict(width=128, height=96, bits=8, seed=77), dict(sigma=3.0, bt=0)),
+    ("bt1", dict(width=128, height=96, bits=8, seed=78), dict(sigma=3.0, bt=1, sharpen=0.2)),
+    ("sharpen_only", dict(width=128, height=96, bits=8, seed=79), dict(sigma=3.0, bt=-1, sharpen=0.4)),
+]
+
+
+def _clip(torch, clip):
+    planes = synth.make_clip(frames=F, noise_sigma=5.0 * (4 if clip["bits"] == 10 else 1), **clip)
+    dev = [torch.from_numpy(a.astype(np.int16) if a.dtype == np.uint16 else a).cuda() for a in planes]
+    return planes, dev
+
+
+def _engines(planes, clip, filt):
+    p = make_params(**filt)
+    descs = plane_descs([a.shape[1:] for a in planes], clip["bits"], F)
+    engs = [engine.PlaneEngine(p, d) for d in descs]
+    if filt.get("pfactor"):
+        for e, a in zip(engs, planes):
+            e.set_pattern_frame(a[filt["pframe"]])
+    return engs
+
+
+def _ptr(a, n):
+    fb = a.shape[1] * a.shape[2] * a.element_size()
+    return a.data_ptr() + n * fb if 0 <= n < a.shape[0] else 0
+
+
+def _per_frame(torch, planes, dev, clip, filt):
+    engs = _engines(planes, clip, filt)
+    outs = []
+    for e, a in zip(engs, dev):
+        o = torch.empty_like(a)
+        st = a.shape[2] * a.element_size()
+        for n in range(F):
+            e.filter_device(n, [_ptr(a, n + d) for d in range(-2, 3)], [st] * 5, _ptr(o, n), st, 0)
+        outs.append(o)
+        e.close()
+    torch.cuda.synchronize()
+    return [o.cpu().numpy() for o in outs]
+
+
+def _grouped(torch, planes, dev, clip, filt, sizes):
+    """Frames in groups of the given sizes (cycled) per plane."""
+    engs = _engines(planes, clip, filt)
+    outs = []
+    for e, a in zip(engs, dev):
+        o = torch.empty_like(a)
+        st = a.shape[2] * a.element_size()
+        n0, i = 0, 0
+        while n0 < F:
+            k = min(sizes[i % len(sizes)], F - n0)
+            e.filter_frames_device(n0, [_ptr(a, n) for n in range(n0 - 2, n0 + k + 2)], [st] * (k + 4),
+                                   [_ptr(o, n) for n in range(n0, n0 + k)], [st] * k, 0)
+            n0 += k
+            i += 1
+        outs.append(o)
+        e.close()
+    torch.cuda.synchronize()
+    return [o.cpu().numpy() for o in outs]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,clip,filt", CASES, ids=[c[0] for c in CASES])
+def test_frame_groups_match_per_frame(gpu, name, clip, filt):
+    import torch
+    planes, dev = _clip(torch, clip)
+    ref = _per_frame(torch, planes, dev, clip, filt)
+    for sizes in ([4], [16], [3, 1, 7, 2]):
+        got = _grouped(torch, planes, dev, clip, filt, sizes)
+        for i, (r, g) in enumerate(zip(ref, got)):
+            assert np.array_equal(r, g), (name, sizes, i, int(np.abs(r.astype(int) - g).max()))
+
+
+@pytest.mark.gpu
+def test_frame_groups_tensor_core_path(gpu, monkeypatch):
+    """The tensor-core path takes frame groups one frame at a time."""
+    import torch
+    monkeypatch.setenv("NEO_FFT3D_PATH", "tc")
+    clip, filt = CASES[0][1], CASES[0][2]
+    planes, dev = _clip(torch, clip)
+    ref = _per_frame(torch, planes, dev, clip, filt)
+    got = _grouped(torch, planes, dev, clip, filt, [5])
+    for r, g in zip(ref, got):
+        assert np.array_equal(r, g)
+
+
+@pytest.mark.gpu
+def test_frame_group_timing_counts_unique_spectra(gpu):
+    """Per-kernel timing of a frame group: one filter/inverse launch whose
+    algorithmic bytes count each window spectrum once."""
+    import torch
+    clip, filt = CASES[0][1], CASES[0][2]
+    planes, dev = _clip(torch, clip)
+    e = _engines(planes[:1], clip, filt)[0]
+    a = dev[0]
+    o = torch.empty_like(a)
+    st = a.shape[2]
+    e.filter_frames_device(4, [_ptr(a, n) for n in range(2, 12)], [st] * 10, [_ptr(o, n) for n in range(4, 10)],
+                           [st] * 6, 0)  # warm: frames 4..9
+    e.timing()
+    e.set_timing(True)
+    e.filter_frames_device(10, [_ptr(a, n) for n in range(8, 18)], [st] * 10, [_ptr(o, n) for n in range(10, 16)],
+                           [st] * 6, 0)
+    torch.cuda.synchronize()
+    t = e.timing()
+    e.set_timing(False)
+    S = e.nblocks * 32 * 17 * 8
+    T = e.nblocks * 32 * 32 * 4
+    assert t["filter_inverse"][0] == 1
+    assert t["filter_inverse"][2] == pytest.approx(10 * S + 6 * T)  # frames 8..17 once, six outputs
+    assert t["forward"][0] == 6  # frames 12..17 are new
+    e.close()
+
+
+@pytest.mark.gpu
+def test_frame_group_argument_checks(gpu):
+    import torch
+    a = torch.zeros((4, 64, 64), dtype=torch.uint8, device="cuda")
+    e = engine.PlaneEngine(make_params(sigma=2.0, bt=3), plane_descs([(64, 64)], 8, 4)[0])
+    L = engine.lib()
+    import ctypes
+    p = (ctypes.c_void_p * 21)()
+    s = (ctypes.c_int * 21)()
+    d = (ctypes.c_void_p * 17)(*([a.data_ptr()] * 17))
+    ds = (ctypes.c_int * 17)()
+    assert L.fft3d_plane_filter_frames_device(e.h, 0, 17, p, s, d, ds, None) == -1
+    assert "frame group" in L.fft3d_last_error().decode()
+    assert L.fft3d_plane_filter_frames_device(e.h, 0, 0, p, s, d, ds, None) == -1
+    e.close()
