@@ -446,14 +446,21 @@ def main():
     # the engine queues each call and overlaps its copies with other calls' kernels
     E2E_THREADS = 4
 
+    G = head["group"]
+
     def e2e_plane(i, counter, lock):
         e, a, o = engs[i], nps_in[i], nps_out[i]
         while True:
             with lock:
                 n = counter[0]
-                counter[0] += 1
+                counter[0] += max(G, 1)
             if n >= F:
                 return
+            if G:
+                k = min(G, F - n)
+                e.filter_frames(n, [a[m] if 0 <= m < F else None for m in range(n - 2, n + k + 2)],
+                                [o[m] for m in range(n, n + k)])
+                continue
             win = [a[n + d] if 0 <= n + d < F else None for d in range(-2, 3)]
             e.filter(n, win, o[n])
 
@@ -486,8 +493,9 @@ def main():
         frame_bytes = sum(a[0].nbytes for a in planes)
         e2e = {"value": world * F * args.e2e_steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": F * frame_bytes, "d2h_bytes_per_step": F * frame_bytes,
-               "path": f"fft3d_plane_filter (host API), {E2E_THREADS} host threads per plane (frame-parallel), "
-                       "pinned buffers"}
+               "path": (f"fft3d_plane_filter_frames (host API, groups of {G} frames)" if G else
+                        "fft3d_plane_filter (host API)") +
+                       f", {E2E_THREADS} host threads per plane (frame-parallel), pinned buffers"}
 
     kalman = None if args.no_kalman else kalman_4k(args, torch, dist, engine, make_params, plane_descs, local, world)
 

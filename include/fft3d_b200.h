@@ -109,6 +109,15 @@ int fft3d_plane_filter_device(fft3d_plane* h, int n, const void* const src[5], c
 int fft3d_plane_filter_frames_device(fft3d_plane* h, int n0, int count, const void* const* src,
                                      const int* src_stride, void* const* dst, const int* dst_stride, void* stream);
 
+/* Same as fft3d_plane_filter_frames_device with HOST frames (as in
+ * fft3d_plane_filter): the frames the group needs and the device does not
+ * hold are uploaded, the outputs downloaded, and the call returns when they
+ * are in dst. Calls from several threads overlap one call's copies with
+ * another's kernels. Planes with crop borders, and planes that are not
+ * grouped, go through fft3d_plane_filter frame by frame. */
+int fft3d_plane_filter_frames(fft3d_plane* h, int n0, int count, const void* const* src, const int* src_stride,
+                              void* const* dst, const int* dst_stride);
+
 /* 1 if the spectrum of frame n is held in the device spectrum cache. */
 int fft3d_plane_cached(fft3d_plane* h, int n);
 

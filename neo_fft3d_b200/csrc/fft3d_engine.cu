@@ -119,6 +119,22 @@ struct fft3d_plane {
   };
   static constexpr int kStages = 3;
   Stage stages[kStages];
+  // Host frame groups (fft3d_plane_filter_frames): per call, the group's
+  // uploaded frames and its outputs in pitched device planes (grown to the
+  // largest group), used round robin like the one-frame stages.
+  struct GroupStage {
+    // planes of `row` bytes per line, no padding, one after another: frames
+    // that are contiguous in host memory move in one copy
+    char* in = nullptr;
+    char* out = nullptr;
+    int nin = 0, nout = 0;
+    cudaEvent_t in_free = nullptr;   // the kernels reading `in` are done
+    cudaEvent_t out_free = nullptr;  // the downloads of `out` are done
+    int* h_flags = nullptr;          // pinned copy of the device error flag
+  };
+  static constexpr int kGroupStages = 4;
+  GroupStage gstages[kGroupStages];
+  int next_gstage = 0;
   int next_stage = 0;
   Stage* cur = nullptr;            // the stage of the call being queued
   cudaEvent_t call_done = nullptr;  // completion event of the call being queued
@@ -296,6 +312,13 @@ void free_plane(fft3d_plane* P) {
     if (sg.in_free) cudaEventDestroy(sg.in_free);
     if (sg.out_free) cudaEventDestroy(sg.out_free);
     if (sg.h_flags) cudaFreeHost(sg.h_flags);
+  }
+  for (auto& gs : P->gstages) {
+    cudaFree(gs.in);
+    cudaFree(gs.out);
+    if (gs.in_free) cudaEventDestroy(gs.in_free);
+    if (gs.out_free) cudaEventDestroy(gs.out_free);
+    if (gs.h_flags) cudaFreeHost(gs.h_flags);
   }
   for (auto e : P->sync_pool) cudaEventDestroy(e);
   if (P->s_up) cudaStreamDestroy(P->s_up);
@@ -787,6 +810,206 @@ void count_launches(uint64_t n) { g_launches += n; }
 int engine_fail(int code, const std::string& msg) { return fail(code, msg); }
 }  // namespace fft3d
 
+namespace {
+
+int check_group_args(const fft3d_plane* P, int count, const void* const* src, const int* src_stride,
+                     void* const* dst, const int* dst_stride) {
+  if (!P || !src || !src_stride || !dst || !dst_stride || count < 1 || count > FFT3D_MAX_FRAME_GROUP)
+    return fail(FFT3D_E_PARAM, "neo_fft3d: invalid frame group arguments");
+  for (int j = 0; j < count; j++)
+    if (!dst[j]) return fail(FFT3D_E_PARAM, "neo_fft3d: null output frame in a frame group");
+  return FFT3D_OK;
+}
+
+// Whether a call of `count` frames runs as a frame group: Wiener 3D planes on
+// the default path (Kalman state runs frame to frame; bt = 1 and sharpen-only
+// windows share no spectra).
+bool group_path(const fft3d_plane* P, int count) {
+  return count > 1 && P->ep.bt >= 2 && fft3d::plane_batchable(P).empty();
+}
+
+// Frames n0 .. n0 + count - 1 from device frames (the window of frame n0 + j
+// is src[j .. j + 4]), queued on st; the caller holds P->mu.
+int filter_group(fft3d_plane* P, int n0, int count, const void* const* src, const int* src_stride,
+                 void* const* dst, const int* dst_stride, cudaStream_t st) {
+  if (!group_path(P, count)) {
+    for (int j = 0; j < count; j++) {
+      int rc = run_filter(P, n0 + j, src + j, src_stride + j, dst[j], dst_stride[j], false, st);
+      if (rc) return rc;
+    }
+    return FFT3D_OK;
+  }
+  int lo, hi;
+  group_range(P, n0, count, &lo, &hi);
+  int rc = group_resources(P, lo, hi, count);
+  if (rc) return rc;
+  fft3d::Deferred d;
+  P->keep_lo = lo;
+  P->keep_hi = hi;
+  P->fixed_reverse = (int)(P->groups_done++ & 1);
+  for (int j = 0; j < count && rc == FFT3D_OK; j++) {
+    P->occ = j;
+    d.plane = j;
+    g_defer = &d;
+    rc = run_filter(P, n0 + j, src + j, src_stride + j, dst[j], dst_stride[j], false, st);
+    g_defer = nullptr;
+  }
+  P->occ = 0;
+  P->keep_lo = 1;
+  P->keep_hi = 0;
+  P->fixed_reverse = -1;
+  if (rc) {
+    discard_recorded(P, d);
+    return rc;
+  }
+  return run_group(P, d, st);
+}
+
+// Device planes of a host frame group's stage: `nin` input and `nout`
+// output planes (grown, never shrunk; growing waits for the stage's previous
+// use), its events and its pinned flag.
+int group_stage_size(fft3d_plane* P, fft3d_plane::GroupStage* gs, int nin, int nout) {
+  const size_t plane = (size_t)P->d.width * P->bytes * P->d.height;
+  if (gs->nin < nin || gs->nout < nout) {
+    if (gs->in_free) {
+      cudaEventSynchronize(gs->in_free);
+      cudaEventSynchronize(gs->out_free);
+    }
+    cudaFree(gs->in);
+    cudaFree(gs->out);
+    gs->in = gs->out = nullptr;
+    gs->nin = gs->nout = 0;
+    if (cudaMalloc(&gs->in, plane * nin) != cudaSuccess || cudaMalloc(&gs->out, plane * nout) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (frame group staging)");
+    }
+    gs->nin = nin;
+    gs->nout = nout;
+  }
+  if (!gs->in_free) {
+    if (cudaEventCreateWithFlags(&gs->in_free, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&gs->out_free, cudaEventDisableTiming) != cudaSuccess ||
+        cudaMallocHost(&gs->h_flags, sizeof(int)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(FFT3D_E_CUDA, "neo_fft3d: frame group staging setup failed");
+    }
+    gs->h_flags[0] = 0;
+  }
+  return FFT3D_OK;
+}
+
+// Host frame group: the frames the group needs and the ring lacks go up on
+// the upload stream into the stage's planes, the group runs on the plane's
+// stream, and its outputs come down on the download stream; the plane's
+// lock is held only while the call is queued (as in fft3d_plane_filter).
+int filter_group_host(fft3d_plane* P, int n0, int count, const void* const* src, const int* src_stride,
+                      void* const* dst, const int* dst_stride) {
+  cudaEvent_t done = nullptr;
+  fft3d_plane::GroupStage* gs = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(P->mu);
+    CK(cudaSetDevice(P->device), "cudaSetDevice");
+    cudaStream_t st = P->stream;
+    gs = &P->gstages[P->next_gstage];
+    P->next_gstage = (P->next_gstage + 1) % fft3d_plane::kGroupStages;
+    int rc = group_stage_size(P, gs, count + 4, count);
+    if (rc) return rc;
+    const size_t row = (size_t)P->d.width * P->bytes;
+    const size_t plane = row * P->d.height;
+    int lo, hi;
+    group_range(P, n0, count, &lo, &hi);
+    lo = std::max(lo, 0);
+    hi = std::min(hi, P->d.num_frames - 1);
+    const void* dsrc[FFT3D_MAX_FRAME_GROUP + 4] = {};
+    int dsstride[FFT3D_MAX_FRAME_GROUP + 4] = {};
+    bool need[FFT3D_MAX_FRAME_GROUP + 4] = {};
+    bool uploads = false;
+    for (int m = lo; m <= hi; m++) {
+      if (find_slot(P, m)) continue;
+      const int k = m - (n0 - 2);
+      if (!src[k])
+        return fail(FFT3D_E_FRAME, "neo_fft3d: frame " + std::to_string(m) + " is needed but was not supplied");
+      need[k] = true;
+      dsrc[k] = gs->in + k * plane;
+      dsstride[k] = (int)row;
+      uploads = true;
+    }
+    if (uploads) {
+      // the kernels that read the stage's previous frames are done
+      CK(cudaStreamWaitEvent(P->s_up, gs->in_free, 0), "event");
+      for (int k = 0; k < count + 4;) {
+        if (!need[k]) {
+          k++;
+          continue;
+        }
+        // a run of frames that are contiguous unpadded planes in host memory
+        // moves in one copy
+        int e = k + 1;
+        if ((size_t)src_stride[k] == row)
+          while (e < count + 4 && need[e] && (size_t)src_stride[e] == row &&
+                 static_cast<const char*>(src[e]) == static_cast<const char*>(src[e - 1]) + plane)
+            e++;
+        if (e - k > 1)
+          CK(cudaMemcpyAsync(gs->in + k * plane, src[k], plane * (e - k), cudaMemcpyHostToDevice, P->s_up),
+             "frame upload");
+        else
+          CK(cudaMemcpy2DAsync(gs->in + k * plane, row, src[k], src_stride[k], row, P->d.height,
+                               cudaMemcpyHostToDevice, P->s_up),
+             "frame upload");
+        k = e;
+      }
+    }
+    if (uploads) {
+      rc = stream_after(P, st, P->s_up);
+      if (rc) return rc;
+    }
+    // the stage's previous outputs must have been downloaded
+    CK(cudaStreamWaitEvent(st, gs->out_free, 0), "event");
+    void* ddst[FFT3D_MAX_FRAME_GROUP];
+    int ddstride[FFT3D_MAX_FRAME_GROUP];
+    for (int j = 0; j < count; j++) {
+      ddst[j] = gs->out + j * plane;
+      ddstride[j] = (int)row;
+    }
+    rc = filter_group(P, n0, count, dsrc, dsstride, ddst, ddstride, st);
+    if (rc) return rc;
+    CK(cudaEventRecord(gs->in_free, st), "event");
+    rc = stream_after(P, P->s_down, st);
+    if (rc) return rc;
+    for (int j = 0; j < count;) {
+      int e = j + 1;
+      if ((size_t)dst_stride[j] == row)
+        while (e < count && (size_t)dst_stride[e] == row &&
+               static_cast<char*>(dst[e]) == static_cast<char*>(dst[e - 1]) + plane)
+          e++;
+      if (e - j > 1)
+        CK(cudaMemcpyAsync(dst[j], gs->out + j * plane, plane * (e - j), cudaMemcpyDeviceToHost, P->s_down),
+           "result download");
+      else
+        CK(cudaMemcpy2DAsync(dst[j], dst_stride[j], gs->out + j * plane, row, row, P->d.height,
+                             cudaMemcpyDeviceToHost, P->s_down),
+           "result download");
+      j = e;
+    }
+    CK(cudaEventRecord(gs->out_free, P->s_down), "event");
+    gs->h_flags[0] = 0;
+    CK(cudaMemcpyAsync(gs->h_flags, P->d_err, sizeof(int), cudaMemcpyDeviceToHost, P->s_down), "error flag");
+    done = take_sync_event(P);
+    CK(cudaEventRecord(done, P->s_down), "event");
+  }
+  cudaSetDevice(P->device);
+  const cudaError_t e = cudaEventSynchronize(done);
+  give_sync_event(P, done);
+  if (e != cudaSuccess) return cuda_fail(e, "synchronize");
+  if (gs->h_flags[0]) {
+    cudaMemset(P->d_err, 0, sizeof(int));
+    return fail(FFT3D_E_CUDA, "neo_fft3d: a bounded completion wait timed out");
+  }
+  return FFT3D_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 void fft3d_params_default(fft3d_params* p) {
@@ -1068,45 +1291,29 @@ int fft3d_plane_filter_device(fft3d_plane* P, int n, const void* const src[5], c
 
 int fft3d_plane_filter_frames_device(fft3d_plane* P, int n0, int count, const void* const* src, const int* src_stride,
                                      void* const* dst, const int* dst_stride, void* stream) {
-  if (!P || !src || !src_stride || !dst || !dst_stride || count < 1 || count > FFT3D_MAX_FRAME_GROUP)
-    return fail(FFT3D_E_PARAM, "neo_fft3d: invalid frame group arguments");
-  for (int j = 0; j < count; j++)
-    if (!dst[j]) return fail(FFT3D_E_PARAM, "neo_fft3d: null output frame in a frame group");
+  int rc = check_group_args(P, count, src, src_stride, dst, dst_stride);
+  if (rc) return rc;
   std::lock_guard<std::mutex> lk(P->mu);
   CK(cudaSetDevice(P->device), "cudaSetDevice");
-  cudaStream_t st = stream ? (cudaStream_t)stream : P->stream;
-  // frame n0 + j reads the window src[j .. j + 4]
-  if (count == 1 || P->ep.bt < 2 || !fft3d::plane_batchable(P).empty()) {
-    for (int j = 0; j < count; j++) {
-      int rc = run_filter(P, n0 + j, src + j, src_stride + j, dst[j], dst_stride[j], false, st);
-      if (rc) return rc;
-    }
-    return FFT3D_OK;
-  }
-  int lo, hi;
-  group_range(P, n0, count, &lo, &hi);
-  int rc = group_resources(P, lo, hi, count);
+  return filter_group(P, n0, count, src, src_stride, dst, dst_stride, stream ? (cudaStream_t)stream : P->stream);
+}
+
+int fft3d_plane_filter_frames(fft3d_plane* P, int n0, int count, const void* const* src, const int* src_stride,
+                              void* const* dst, const int* dst_stride) {
+  int rc = check_group_args(P, count, src, src_stride, dst, dst_stride);
   if (rc) return rc;
-  fft3d::Deferred d;
-  P->keep_lo = lo;
-  P->keep_hi = hi;
-  P->fixed_reverse = (int)(P->groups_done++ & 1);
-  for (int j = 0; j < count && rc == FFT3D_OK; j++) {
-    P->occ = j;
-    d.plane = j;
-    g_defer = &d;
-    rc = run_filter(P, n0 + j, src + j, src_stride + j, dst[j], dst_stride[j], false, st);
-    g_defer = nullptr;
+  bool grouped;
+  {
+    std::lock_guard<std::mutex> lk(P->mu);
+    // crop borders are copied from the host frames by the one-frame host path
+    grouped = group_path(P, count) && P->ep.l == 0 && P->ep.t == 0 && P->ep.r == 0 && P->ep.b == 0;
   }
-  P->occ = 0;
-  P->keep_lo = 1;
-  P->keep_hi = 0;
-  P->fixed_reverse = -1;
-  if (rc) {
-    discard_recorded(P, d);
-    return rc;
+  if (grouped) return filter_group_host(P, n0, count, src, src_stride, dst, dst_stride);
+  for (int j = 0; j < count; j++) {
+    rc = fft3d_plane_filter(P, n0 + j, src + j, src_stride + j, dst[j], dst_stride[j]);
+    if (rc) return rc;
   }
-  return run_group(P, d, st);
+  return FFT3D_OK;
 }
 
 int fft3d_plane_cached(fft3d_plane* P, int n) {

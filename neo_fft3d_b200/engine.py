@@ -43,6 +43,8 @@ def lib():
         L.fft3d_plane_filter_device.argtypes = [vp, ci, ctypes.POINTER(vp), ctypes.POINTER(ci), vp, ci, vp]
         L.fft3d_plane_filter_frames_device.argtypes = [vp, ci, ci, ctypes.POINTER(vp), ctypes.POINTER(ci),
                                                        ctypes.POINTER(vp), ctypes.POINTER(ci), vp]
+        L.fft3d_plane_filter_frames.argtypes = [vp, ci, ci, ctypes.POINTER(vp), ctypes.POINTER(ci),
+                                                ctypes.POINTER(vp), ctypes.POINTER(ci)]
         L.fft3d_plane_cached.argtypes = [vp, ci]
         L.fft3d_plane_spectrum.argtypes = [vp, ci, vp]
         L.fft3d_plane_geometry.argtypes = [vp, ctypes.POINTER(ci)]
@@ -122,6 +124,20 @@ class PlaneEngine:
         ds = (ctypes.c_int * count)(*dst_strides)
         _check(lib().fft3d_plane_filter_frames_device(self.h, n0, count, p, s, d, ds,
                                                       ctypes.c_void_p(stream) if stream else None))
+
+    def filter_frames(self, n0: int, srcs, dsts):
+        """Filter frames n0 .. n0 + len(dsts) - 1 from host frames in one call
+        (a frame group): srcs[j] is frame n0 - 2 + j (len(dsts) + 4 entries,
+        None outside the clip or when cached), dsts[j] receives frame n0 + j
+        (2D arrays, rows contiguous)."""
+        count = len(dsts)
+        if len(srcs) != count + 4:
+            raise ValueError("filter_frames: srcs needs len(dsts) + 4 entries")
+        p = (ctypes.c_void_p * (count + 4))(*[None if a is None else a.ctypes.data for a in srcs])
+        s = (ctypes.c_int * (count + 4))(*[0 if a is None else a.strides[0] for a in srcs])
+        d = (ctypes.c_void_p * count)(*[a.ctypes.data for a in dsts])
+        ds = (ctypes.c_int * count)(*[a.strides[0] for a in dsts])
+        _check(lib().fft3d_plane_filter_frames(self.h, n0, count, p, s, d, ds))
 
     def cached(self, n: int) -> bool:
         return bool(lib().fft3d_plane_cached(self.h, n))

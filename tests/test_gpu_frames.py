@@ -150,3 +150,81 @@ def test_frame_group_argument_checks(gpu):
     assert "frame group" in L.fft3d_last_error().decode()
     assert L.fft3d_plane_filter_frames_device(e.h, 0, 0, p, s, d, ds, None) == -1
     e.close()
+
+
+def _host_per_frame(planes, clip, filt):
+    engs = _engines(planes, clip, filt)
+    outs = []
+    for e, a in zip(engs, planes):
+        o = np.empty_like(a)
+        for n in range(F):
+            e.filter(n, [a[n + d] if 0 <= n + d < F else None for d in range(-2, 3)], o[n])
+        outs.append(o)
+        e.close()
+    return outs
+
+
+def _host_grouped(planes, clip, filt, sizes):
+    engs = _engines(planes, clip, filt)
+    outs = []
+    for e, a in zip(engs, planes):
+        o = np.empty_like(a)
+        n0, i = 0, 0
+        while n0 < F:
+            k = min(sizes[i % len(sizes)], F - n0)
+            e.filter_frames(n0, [a[n] if 0 <= n < F else None for n in range(n0 - 2, n0 + k + 2)],
+                            [o[n] for n in range(n0, n0 + k)])
+            n0 += k
+            i += 1
+        outs.append(o)
+        e.close()
+    return outs
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["bt5_sharpen", "bt5_10bit", "bt3_crop_dehalo", "kalman"])
+def test_host_frame_groups_match_per_frame(gpu, name):
+    """Host buffers: frame groups (uploads of only the missing frames,
+    downloads of the group's outputs) equal the one-frame host path."""
+    clip, filt = next((c[1], c[2]) for c in CASES if c[0] == name)
+    planes = synth.make_clip(frames=F, noise_sigma=5.0 * (4 if clip["bits"] == 10 else 1), **clip)
+    ref = _host_per_frame(planes, clip, filt)
+    for sizes in ([8], [3, 5, 16]):
+        got = _host_grouped(planes, clip, filt, sizes)
+        for i, (r, g) in enumerate(zip(ref, got)):
+            assert np.array_equal(r, g), (name, sizes, i)
+
+
+@pytest.mark.gpu
+def test_host_frame_groups_from_threads(gpu):
+    """Several host threads taking groups of one plane from a shared counter
+    (as the bench's end-to-end arm does): the outputs equal a serial run."""
+    import threading
+    clip, filt = CASES[0][1], CASES[0][2]
+    planes = synth.make_clip(frames=F, noise_sigma=5.0, **clip)
+    ref = _host_grouped(planes, clip, filt, [4])
+    engs = _engines(planes, clip, filt)
+    outs = [np.empty_like(a) for a in planes]
+    for e, a, o in zip(engs, planes, outs):
+        counter, lock = [0], threading.Lock()
+
+        def work():
+            while True:
+                with lock:
+                    n0 = counter[0]
+                    counter[0] += 4
+                if n0 >= F:
+                    return
+                k = min(4, F - n0)
+                e.filter_frames(n0, [a[n] if 0 <= n < F else None for n in range(n0 - 2, n0 + k + 2)],
+                                [o[n] for n in range(n0, n0 + k)])
+
+        th = [threading.Thread(target=work) for _ in range(4)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+    for r, g in zip(ref, outs):
+        assert np.array_equal(r, g)
+    for e in engs:
+        e.close()
