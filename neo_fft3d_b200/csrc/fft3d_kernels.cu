@@ -93,7 +93,98 @@ __device__ __forceinline__ void overlap_add_px(const OlaArgs& a, int x0, int k) 
   store_sample<T>(row + x0, v, a.maxval);
 }
 
+// Four adjacent output pixels per thread (x0 a multiple of 4), for planes
+// whose block step, overlap, width and block width are multiples of 4 and
+// whose destination rows are aligned for a 4-sample store: the four pixels
+// share their blocks and overlap case, so the tdom reads are float4 loads,
+// the block indices are computed once and the samples go out in one store.
+// Each pixel's arithmetic is overlap_add_px's, term for term.
+template <typename T>
+struct Pack4;
+template <>
+struct Pack4<uint8_t> {
+  using V = uchar4;
+};
+template <>
+struct Pack4<uint16_t> {
+  using V = ushort4;
+};
+template <>
+struct Pack4<float> {
+  using V = float4;
+};
+
+template <typename T>
+__device__ __forceinline__ T clamp_sample(float v, int maxval) {
+  if constexpr (sizeof(T) == 4) {
+    float c = v < 0.f ? 0.f : v;
+    return c > 1.f ? 1.f : c;
+  } else {
+    int i = __float2int_rz(v);
+    i = i < 0 ? 0 : (i > maxval ? maxval : i);
+    return (T)i;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void overlap_add_px4(const OlaArgs& a, int x0, int k) {
+  const Geom& g = a.g;
+  if (x0 >= g.W || k >= g.H) return;
+  const int Y = g.sy + k, X = g.sx + x0;
+  const int by = Y / g.sy, y = Y - by * g.sy;
+  const int bx = X / g.sx, x = X - bx * g.sx;
+  const bool yov = y < g.oh, xov = x < g.ow;
+  const int bw = g.bw, bh = g.bh;
+  auto at4 = [&](int bxx, int byy, int yy, int xx) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(a.tdom + ((size_t)(byy * g.nox + bxx) * bh + yy) * bw + xx));
+    return q;
+  };
+  auto comp = [](const float4& q, int i) { return i == 0 ? q.x : (i == 1 ? q.y : (i == 2 ? q.z : q.w)); };
+  const float norm = a.norm;
+  float v[4];
+  if (!yov) {
+    const float4 d = at4(bx, by, y, x);
+    if (!xov) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) v[i] = comp(d, i) * norm + a.rounder + a.base;
+    } else {
+      const float4 c = at4(bx - 1, by, y, x + g.sx);
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+        v[i] = (comp(c, i) * __ldg(a.t.wsyn_xr + x + i) + comp(d, i) * __ldg(a.t.wsyn_xl + x + i)) * norm + a.rounder +
+               a.base;
+    }
+  } else {
+    const float wr = __ldg(a.t.wsyn_yr + y) * norm, wl = __ldg(a.t.wsyn_yl + y) * norm;
+    const float4 b = at4(bx, by - 1, y + g.sy, x), d = at4(bx, by, y, x);
+    if (!xov) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) v[i] = (comp(b, i) * wr + comp(d, i) * wl) + a.rounder + a.base;
+    } else {
+      const float4 aa = at4(bx - 1, by - 1, y + g.sy, x + g.sx), c = at4(bx - 1, by, y, x + g.sx);
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const float sxr = __ldg(a.t.wsyn_xr + x + i), sxl = __ldg(a.t.wsyn_xl + x + i);
+        v[i] = ((comp(aa, i) * sxr + comp(b, i) * sxl) * wr + (comp(c, i) * sxr + comp(d, i) * sxl) * wl) + a.rounder +
+               a.base;
+      }
+    }
+  }
+  T* row = reinterpret_cast<T*>(static_cast<char*>(a.dst) + (long long)field_row(k, g.H, g.interlaced) * a.dst_stride);
+  typename Pack4<T>::V o;
+  o.x = clamp_sample<T>(v[0], a.maxval);
+  o.y = clamp_sample<T>(v[1], a.maxval);
+  o.z = clamp_sample<T>(v[2], a.maxval);
+  o.w = clamp_sample<T>(v[3], a.maxval);
+  *reinterpret_cast<typename Pack4<T>::V*>(row + x0) = o;
+}
+
 constexpr int kOlaTx = 32, kOlaTy = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(kOlaTx * kOlaTy) k_overlap_add4(OlaArgs a) {
+  overlap_add_px4<T>(a, 4 * (blockIdx.x * blockDim.x + threadIdx.x), blockIdx.y * blockDim.y + threadIdx.y);
+}
 
 template <typename T>
 __global__ void __launch_bounds__(kOlaTx * kOlaTy) k_overlap_add(OlaArgs a) {
@@ -275,6 +366,16 @@ int batch_occupancy(int bw, int bh, int which, int mode_or_bytes) {
 
 cudaError_t launch_overlap_add(const OlaArgs& a, int bytes, cudaStream_t s) {
   dim3 block(kOlaTx, kOlaTy);
+  const bool four = a.g.sx % 4 == 0 && a.g.ow % 4 == 0 && a.g.W % 4 == 0 && a.g.bw % 4 == 0 &&
+                    reinterpret_cast<uintptr_t>(a.tdom) % 16 == 0 &&
+                    reinterpret_cast<uintptr_t>(a.dst) % (4 * bytes) == 0 && a.dst_stride % (4 * bytes) == 0;
+  if (four) {
+    dim3 grid((a.g.W / 4 + kOlaTx - 1) / kOlaTx, (a.g.H + kOlaTy - 1) / kOlaTy);
+    if (bytes == 1) k_overlap_add4<uint8_t><<<grid, block, 0, s>>>(a);
+    else if (bytes == 2) k_overlap_add4<uint16_t><<<grid, block, 0, s>>>(a);
+    else k_overlap_add4<float><<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+  }
   dim3 grid((a.g.W + kOlaTx - 1) / kOlaTx, (a.g.H + kOlaTy - 1) / kOlaTy);
   if (bytes == 1) k_overlap_add<uint8_t><<<grid, block, 0, s>>>(a);
   else if (bytes == 2) k_overlap_add<uint16_t><<<grid, block, 0, s>>>(a);
