@@ -707,10 +707,24 @@ int run_group(fft3d_plane* P, const fft3d::Deferred& d, cudaStream_t st) {
   const double S = (double)P->spec_elems() * sizeof(float2);
   const double T = (double)P->g.nblocks * P->g.bh * P->g.bw * 4;
   const double pix = (double)P->g.W * P->g.H * P->bytes;
-  for (const auto& f : d.fwd) {
-    TimeScope ts(P, K_FORWARD, pix + S, st);
-    CK(fft3d::launch_forward(f.a, f.bytes, st), "forward kernel");
+  // the new frames' forward transforms: one launch for all of them
+  for (size_t i = 0; i < d.fwd.size();) {
+    const size_t e = std::min(d.fwd.size(), i + (size_t)fft3d::kMaxFwdFrames);
+    TimeScope ts(P, K_FORWARD, (double)(e - i) * (pix + S), st);
+    if (e - i == 1) {
+      CK(fft3d::launch_forward(d.fwd[i].a, d.fwd[i].bytes, st), "forward kernel");
+    } else {
+      fft3d::FwdFrameSet fs{};
+      fs.count = (int)(e - i);
+      for (size_t k = i; k < e; k++) {
+        fs.src[k - i] = d.fwd[k].a.src;
+        fs.stride[k - i] = d.fwd[k].a.src_stride;
+        fs.spec[k - i] = d.fwd[k].a.spec;
+      }
+      CK(fft3d::launch_forward_frames(d.fwd[i].a, fs, d.fwd[i].bytes, st), "forward kernel (frame group)");
+    }
     g_launches++;
+    i = e;
   }
   for (size_t i = 0; i < d.inv.size();) {
     const int mode = d.inv[i].mode;

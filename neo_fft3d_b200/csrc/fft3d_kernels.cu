@@ -244,6 +244,11 @@ cudaError_t launch_filter_inverse(const InverseArgs& a, int mode, cudaStream_t s
   return e ? e->inv(a, mode, s) : cudaErrorInvalidValue;
 }
 
+cudaError_t launch_forward_frames(const ForwardArgs& a, const FwdFrameSet& fs, int bytes, cudaStream_t s) {
+  const SizeEntry* e = find_size(a.g.bw, a.g.bh);
+  return e ? e->fwd_frames(a, fs, bytes, s) : cudaErrorInvalidValue;
+}
+
 cudaError_t launch_filter_inverse_frames(const InverseArgs& a, const FrameSet& fs, int mode, cudaStream_t s) {
   const SizeEntry* e = find_size(a.g.bw, a.g.bh);
   return e ? e->inv_frames(a, fs, mode, s) : cudaErrorInvalidValue;

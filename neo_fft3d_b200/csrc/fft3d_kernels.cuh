@@ -103,6 +103,18 @@ struct FrameSet {
   int count;
 };
 
+// The new frames of a frame group, transformed by one launch: frame j's
+// samples (src/stride as in ForwardArgs) and ring slot. ctas: CTAs per frame
+// (set by the launcher).
+constexpr int kMaxFwdFrames = kMaxGroupFrames + 4;
+struct FwdFrameSet {
+  const void* src[kMaxFwdFrames];
+  long long stride[kMaxFwdFrames];
+  float2* spec[kMaxFwdFrames];
+  int count;
+  int ctas;
+};
+
 // Forward transform of the window's newest frame fused with the filter and
 // the inverse transform (k_fused). f.src/f.spec: the newest frame and its ring
 // slot; v.in[]: the window's spectra (the newest frame's entry is f.spec).
@@ -148,6 +160,9 @@ cudaError_t launch_filter_inverse(const InverseArgs& a, int mode, cudaStream_t s
 // Frame group: fs.count consecutive output frames of one plane (Wiener 3D,
 // mode 2..5) in one launch; a holds everything they share.
 cudaError_t launch_filter_inverse_frames(const InverseArgs& a, const FrameSet& fs, int mode, cudaStream_t s);
+// Forward transforms of fs.count frames of one plane in one launch; a holds
+// what they share (geometry, windows, sample offset).
+cudaError_t launch_forward_frames(const ForwardArgs& a, const FwdFrameSet& fs, int bytes_per_sample, cudaStream_t s);
 cudaError_t launch_overlap_add(const OlaArgs& a, int bytes_per_sample, cudaStream_t s);
 // Batched forms (work items as in BatchLaunch); OLA items are 32x8-pixel tiles.
 cudaError_t launch_forward_batch(int bw, int bh, const BatchLaunch& l, int bytes_per_sample, cudaStream_t s);

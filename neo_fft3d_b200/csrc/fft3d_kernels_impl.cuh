@@ -88,19 +88,74 @@ __device__ __forceinline__ void load_row(const T* p, float (&r)[BW]) {
 // ---------------------------------------------------------------- block FFT phases
 // Sb points at one block's bh x (bw/2+1) complex tile in shared memory.
 
-// Row y of block `blk`: gather (mirrored at the plane edges), analysis window,
-// r2c along x into row y of Sb.
-template <int BW, int BH, typename T>
-__device__ __forceinline__ void fwd_row(const ForwardArgs& a, int blk, int y, float2* Sb) {
-  constexpr int NH = BW / 2 + 1;
+// Where a forward CTA reads its frame and writes its spectra: the launch
+// arguments (one frame per launch), or pointers picked for one frame of a
+// frame group (k_forward_frames).
+struct ArgsFwd {
+  const ForwardArgs& a;
+  __device__ __forceinline__ const void* src() const { return a.src; }
+  __device__ __forceinline__ long long stride() const { return a.src_stride; }
+  __device__ __forceinline__ float2* spec() const { return a.spec; }
+};
+struct FrameFwd {
+  const void* s;
+  long long st;
+  float2* sp;
+  __device__ __forceinline__ const void* src() const { return s; }
+  __device__ __forceinline__ long long stride() const { return st; }
+  __device__ __forceinline__ float2* spec() const { return sp; }
+};
+
+// Source row of row y of block `blk` and the source column of its column 0.
+template <typename T, class Win>
+__device__ __forceinline__ const T* fwd_row_src(const ForwardArgs& a, const Win& win, int blk, int y, int* x0) {
   const Geom& g = a.g;
   const int by = blk / g.nox, bx = blk - by * g.nox;
   const int k = reflect101(by * g.sy + y - g.sy, g.H);
-  const T* srow = reinterpret_cast<const T*>(static_cast<const char*>(a.src) +
-                                             (long long)field_row(k, g.H, g.interlaced) * a.src_stride);
-  const int x0 = bx * g.sx - g.sx;  // source column of block column 0
+  *x0 = bx * g.sx - g.sx;
+  return reinterpret_cast<const T*>(static_cast<const char*>(win.src()) +
+                                    (long long)field_row(k, g.H, g.interlaced) * win.stride());
+}
+
+// Rows whose BW samples are whole 16-byte vectors (8- and 16-bit samples) can
+// be fetched raw ahead of their transform (forward_cta's prefetch).
+template <int BW, typename T>
+__host__ __device__ constexpr int raw_vectors() {
+  return (sizeof(T) <= 2 && (BW * (int)sizeof(T)) % 16 == 0) ? BW * (int)sizeof(T) / 16 : 0;
+}
+
+template <int BW, typename T>
+__device__ __forceinline__ void decode_row(const uint4* raw, float (&r)[BW]) {
+  constexpr int PER = 16 / (int)sizeof(T);
+#pragma unroll
+  for (int v = 0; v < raw_vectors<BW, T>(); v++) {
+    const uint32_t w[4] = {raw[v].x, raw[v].y, raw[v].z, raw[v].w};
+#pragma unroll
+    for (int j = 0; j < PER; j++) {
+      float f;
+      if constexpr (sizeof(T) == 1) f = (float)((w[j >> 2] >> (8 * (j & 3))) & 0xffu);
+      else f = (float)((w[j >> 1] >> (16 * (j & 1))) & 0xffffu);
+      r[v * PER + j] = f;
+    }
+  }
+}
+
+// Row y of block `blk`: gather (mirrored at the plane edges), analysis window,
+// r2c along x into row y of Sb. `raw`: the row's samples already fetched
+// (interior aligned rows), or null.
+template <int BW, int BH, typename T, class Win>
+__device__ __forceinline__ void fwd_row(const ForwardArgs& a, const Win& win, int blk, int y, float2* Sb,
+                                        const uint4* raw) {
+  constexpr int NH = BW / 2 + 1;
+  const Geom& g = a.g;
+  int x0;
+  const T* srow = fwd_row_src<T>(a, win, blk, y, &x0);
   float r[BW];
-  if (x0 >= 0 && x0 + BW <= g.W) {
+  if constexpr (raw_vectors<BW, T>() > 0) {
+    if (raw) decode_row<BW, T>(raw, r);
+  }
+  if (raw_vectors<BW, T>() > 0 && raw) {
+  } else if (x0 >= 0 && x0 + BW <= g.W) {
     load_row<T, BW>(srow + x0, r);
   } else {
 #pragma unroll
@@ -201,8 +256,10 @@ __device__ __forceinline__ void store_tdom(const float2* Sb, float* out, int lan
 
 // One warp transforms blocks_per_warp<BW>() consecutive blocks (rows, then
 // columns, then a coalesced 16-byte copy-out of the contiguous spectra).
-template <int BW, int BH, typename T>
-__device__ __forceinline__ void forward_cta(const ForwardArgs& a, int cta) {
+// PREFETCH: fetch every row of the lane before the first transform (more
+// registers; off where the kernel's register budget is tight).
+template <int BW, int BH, typename T, bool PREFETCH, class Win>
+__device__ __forceinline__ void forward_cta_w(const ForwardArgs& a, int cta, const Win& win) {
   constexpr int NH = BW / 2 + 1, HC = BW / 2, NBW = blocks_per_warp<BW>(), BINS = BH * NH;
   extern __shared__ float2 smem2[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -210,9 +267,39 @@ __device__ __forceinline__ void forward_cta(const ForwardArgs& a, int cta) {
   const Geom& g = a.g;
   const int blk0 = (cta * kWarps + warp) * NBW;
   if (blk0 >= g.nblocks) return;
-  for (int t = lane; t < NBW * BH; t += 32) {
-    const int b = t / BH, y = t - b * BH;
-    if (blk0 + b < g.nblocks) fwd_row<BW, BH, T>(a, blk0 + b, y, S + b * BINS);
+  constexpr int RPL = (NBW * BH + 31) / 32;  // rows per lane
+  constexpr int NV = PREFETCH ? raw_vectors<BW, T>() : 0;
+  if constexpr (NV > 0) {
+    // every row of the lane fetched before the first transform: one load
+    // latency per warp instead of one per row
+    uint4 raw[RPL][NV];
+    bool have[RPL];
+#pragma unroll
+    for (int i = 0; i < RPL; i++) {
+      const int t = lane + 32 * i, b = t / BH, y = t - b * BH;
+      have[i] = false;
+      if (t < NBW * BH && blk0 + b < g.nblocks) {
+        int x0;
+        const T* srow = fwd_row_src<T>(a, win, blk0 + b, y, &x0);
+        const T* p = srow + x0;
+        if (x0 >= 0 && x0 + BW <= g.W && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+#pragma unroll
+          for (int v = 0; v < NV; v++) raw[i][v] = __ldg(reinterpret_cast<const uint4*>(p) + v);
+          have[i] = true;
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < RPL; i++) {
+      const int t = lane + 32 * i, b = t / BH, y = t - b * BH;
+      if (t < NBW * BH && blk0 + b < g.nblocks)
+        fwd_row<BW, BH, T>(a, win, blk0 + b, y, S + b * BINS, have[i] ? raw[i] : nullptr);
+    }
+  } else {
+    for (int t = lane; t < NBW * BH; t += 32) {
+      const int b = t / BH, y = t - b * BH;
+      if (blk0 + b < g.nblocks) fwd_row<BW, BH, T>(a, win, blk0 + b, y, S + b * BINS, nullptr);
+    }
   }
   __syncwarp();
   for (int t = lane; t < NBW * HC; t += 32) {
@@ -221,15 +308,37 @@ __device__ __forceinline__ void forward_cta(const ForwardArgs& a, int cta) {
   }
   __syncwarp();
   const int nvalid = min(NBW, g.nblocks - blk0);
-  float4* dst = reinterpret_cast<float4*>(a.spec + (size_t)blk0 * BINS);
+  float4* dst = reinterpret_cast<float4*>(win.spec() + (size_t)blk0 * BINS);
   const float4* src = reinterpret_cast<const float4*>(S);
   for (int i = lane; i < nvalid * BINS / 2; i += 32) dst[i] = src[i];
   __syncwarp();  // S is reused by the warp's next work item
 }
 
+template <int BW, int BH, typename T, bool PREFETCH = true>
+__device__ __forceinline__ void forward_cta(const ForwardArgs& a, int cta) {
+  forward_cta_w<BW, BH, T, PREFETCH, ArgsFwd>(a, cta, ArgsFwd{a});
+}
+
 template <int BW, int BH, typename T>
 __global__ void __launch_bounds__(kWarps * 32) k_forward(ForwardArgs a) {
   forward_cta<BW, BH, T>(a, blockIdx.x);
+}
+
+// The new frames of a frame group in one launch: CTA x transforms CTA
+// x % fs.ctas of frame x / fs.ctas (one launch instead of one per frame, so
+// the grid has no per-frame wave tail).
+template <int BW, int BH, typename T>
+__global__ void __launch_bounds__(kWarps * 32) k_forward_frames(ForwardArgs a, FwdFrameSet fs) {
+  const int j = blockIdx.x / fs.ctas, c = blockIdx.x - j * fs.ctas;
+  FrameFwd w{nullptr, 0, nullptr};
+#pragma unroll
+  for (int q = 0; q < kMaxFwdFrames; q++)
+    if (q == j) {
+      w.s = fs.src[q];
+      w.st = fs.stride[q];
+      w.sp = fs.spec[q];
+    }
+  forward_cta_w<BW, BH, T, true, FrameFwd>(a, c, w);
 }
 
 // Batched forward: work item i = (plane, CTA of that plane); the grid walks
@@ -241,7 +350,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_forward_batch(const ForwardArgs
     const int2 it = items[i];
     // a private copy: the body's stores cannot alias it, so its fields stay in registers
     const ForwardArgs a = args[it.x];
-    forward_cta<BW, BH, T>(a, it.y);
+    forward_cta<BW, BH, T, false>(a, it.y);
   }
 }
 
@@ -758,7 +867,7 @@ __global__ void __launch_bounds__(kBulkWarps * 32) k_filter_inverse_bulk(Inverse
 template <int BW, int BH, typename T, int MODE>
 __global__ void __launch_bounds__(kWarps * 32, 6) k_fused(FusedArgs A) {
   const int n = fft_ctas<BW, BH>(A.v.g.nblocks);
-  forward_cta<BW, BH, T>(A.f, A.v.reverse ? n - 1 - (int)blockIdx.x : (int)blockIdx.x);
+  forward_cta<BW, BH, T, false>(A.f, A.v.reverse ? n - 1 - (int)blockIdx.x : (int)blockIdx.x);
   filter_inverse_cta<BW, BH, MODE, true>(A.v, blockIdx.x);
 }
 
@@ -915,6 +1024,27 @@ cudaError_t fused_sized(const FusedArgs& a, int mode, int bytes, cudaStream_t s)
   return cudaErrorNotSupported;  // float samples use the unfused path
 }
 
+template <int BW, int BH>
+cudaError_t fwd_frames(const ForwardArgs& a, const FwdFrameSet& fs, int bytes, cudaStream_t s) {
+  if (fs.count < 1 || fs.count > kMaxFwdFrames) return cudaErrorInvalidValue;
+  const int smem = kWarps * fft_smem_bytes<BW, BH>();
+  FwdFrameSet f = fs;
+  f.ctas = fft_grid<BW, BH>(a.g.nblocks);
+  const int grid = f.ctas * f.count;
+  cudaError_t e = cudaSuccess;
+  if (bytes == 1) {
+    e = fft3d::smem_attr(k_forward_frames<BW, BH, uint8_t>, smem);
+    if (e == cudaSuccess) k_forward_frames<BW, BH, uint8_t><<<grid, kWarps * 32, smem, s>>>(a, f);
+  } else if (bytes == 2) {
+    e = fft3d::smem_attr(k_forward_frames<BW, BH, uint16_t>, smem);
+    if (e == cudaSuccess) k_forward_frames<BW, BH, uint16_t><<<grid, kWarps * 32, smem, s>>>(a, f);
+  } else {
+    e = fft3d::smem_attr(k_forward_frames<BW, BH, float>, smem);
+    if (e == cudaSuccess) k_forward_frames<BW, BH, float><<<grid, kWarps * 32, smem, s>>>(a, f);
+  }
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
 template <int BW, int BH, int MODE>
 cudaError_t inv_frames_mode(const InverseArgs& a, const FrameSet& fs, cudaStream_t s) {
   const int smem = kWarps * fft_smem_bytes<BW, BH>();
@@ -959,6 +1089,6 @@ cudaError_t inv_sized(const InverseArgs& a, int mode, cudaStream_t s) {
   static const bool fft3d_reg_##BW##x##BH = register_size(                                             \
       SizeEntry{BW, BH, &fwd_sized<BW, BH>, &inv_sized<BW, BH>, &fused_sized<BW, BH>, &upload_twiddle_table, \
                 &fwd_batch<BW, BH>, &inv_batch<BW, BH>, &ctas_per_plane<BW, BH>, &occupancy_of<BW, BH>,      \
-                &inv_frames<BW, BH>});
+                &inv_frames<BW, BH>, &fwd_frames<BW, BH>});
 
 }  // namespace fft3d

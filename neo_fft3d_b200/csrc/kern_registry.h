@@ -21,6 +21,8 @@ struct SizeEntry {
   int (*occupancy)(int which, int mode_or_bytes);  // resident CTAs per SM: 0 forward, 1 filter/inverse
   // frame groups (Wiener 3D modes 2..5): several output frames in one launch
   cudaError_t (*inv_frames)(const InverseArgs&, const FrameSet&, int mode, cudaStream_t);
+  // and their new frames' forward transforms in one launch
+  cudaError_t (*fwd_frames)(const ForwardArgs&, const FwdFrameSet&, int bytes_per_sample, cudaStream_t);
 };
 
 bool register_size(const SizeEntry& e);

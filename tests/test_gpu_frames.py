@@ -109,8 +109,9 @@ def test_frame_groups_tensor_core_path(gpu, monkeypatch):
 
 @pytest.mark.gpu
 def test_frame_group_timing_counts_unique_spectra(gpu):
-    """Per-kernel timing of a frame group: one filter/inverse launch whose
-    algorithmic bytes count each window spectrum once."""
+    """Per-kernel timing of a frame group: one forward launch for the new
+    frames and one filter/inverse launch whose algorithmic bytes count each
+    window spectrum once."""
     import torch
     clip, filt = CASES[0][1], CASES[0][2]
     planes, dev = _clip(torch, clip)
@@ -131,7 +132,9 @@ def test_frame_group_timing_counts_unique_spectra(gpu):
     T = e.nblocks * 32 * 32 * 4
     assert t["filter_inverse"][0] == 1
     assert t["filter_inverse"][2] == pytest.approx(10 * S + 6 * T)  # frames 8..17 once, six outputs
-    assert t["forward"][0] == 6  # frames 12..17 are new
+    # frames 12..17 are new: transformed by one launch
+    assert t["forward"][0] == 1
+    assert t["forward"][2] == pytest.approx(6 * (a.shape[1] * a.shape[2] + S))
     e.close()
 
 
