@@ -754,11 +754,29 @@ int run_group(fft3d_plane* P, const fft3d::Deferred& d, cudaStream_t st) {
   for (const auto& c : d.copies)
     CK(cudaMemcpy2DAsync(c.dst, c.dpitch, c.src, c.spitch, c.width, c.height, cudaMemcpyDeviceToDevice, st),
        "plane copy");
-  for (const auto& o : d.ola) {
-    TimeScope ts(P, K_OLA, T + pix, st);
-    CK(fft3d::launch_overlap_add(o.a, o.bytes, st), "overlap-add kernel");
-    g_launches++;
+  // the overlap-adds: one launch for all frames where the 4-pixel kernel applies
+  bool merged = false;
+  if (d.ola.size() > 1 && d.ola.size() <= (size_t)fft3d::kMaxGroupFrames) {
+    fft3d::OlaFrameSet fs{};
+    fs.count = (int)d.ola.size();
+    for (size_t k = 0; k < d.ola.size(); k++) {
+      fs.tdom[k] = d.ola[k].a.tdom;
+      fs.dst[k] = d.ola[k].a.dst;
+      fs.dst_stride[k] = d.ola[k].a.dst_stride;
+    }
+    if (fft3d::overlap_add_frames_supported(d.ola[0].a, fs, d.ola[0].bytes)) {
+      TimeScope ts(P, K_OLA, (double)d.ola.size() * (T + pix), st);
+      CK(fft3d::launch_overlap_add_frames(d.ola[0].a, fs, d.ola[0].bytes, st), "overlap-add kernel (frame group)");
+      merged = true;
+      g_launches++;
+    }
   }
+  if (!merged)
+    for (const auto& o : d.ola) {
+      TimeScope ts(P, K_OLA, T + pix, st);
+      CK(fft3d::launch_overlap_add(o.a, o.bytes, st), "overlap-add kernel");
+      g_launches++;
+    }
   return FFT3D_OK;
 }
 

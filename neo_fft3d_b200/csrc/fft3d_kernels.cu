@@ -186,6 +186,21 @@ __global__ void __launch_bounds__(kOlaTx * kOlaTy) k_overlap_add4(OlaArgs a) {
   overlap_add_px4<T>(a, 4 * (blockIdx.x * blockDim.x + threadIdx.x), blockIdx.y * blockDim.y + threadIdx.y);
 }
 
+// Frame blockIdx.z of a frame group (fs): its blocks and destination.
+template <typename T>
+__global__ void __launch_bounds__(kOlaTx * kOlaTy) k_overlap_add4_frames(OlaArgs a, OlaFrameSet fs) {
+  const int j = blockIdx.z;
+  OlaArgs b = a;
+#pragma unroll
+  for (int q = 0; q < kMaxGroupFrames; q++)
+    if (q == j) {
+      b.tdom = fs.tdom[q];
+      b.dst = fs.dst[q];
+      b.dst_stride = fs.dst_stride[q];
+    }
+  overlap_add_px4<T>(b, 4 * (blockIdx.x * blockDim.x + threadIdx.x), blockIdx.y * blockDim.y + threadIdx.y);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kOlaTx * kOlaTy) k_overlap_add(OlaArgs a) {
   overlap_add_px<T>(a, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y);
@@ -367,6 +382,25 @@ int batch_occupancy(int bw, int bh, int which, int mode_or_bytes) {
   }
   const SizeEntry* e = find_size(bw, bh);
   return e ? e->occupancy(which, mode_or_bytes) : 1;
+}
+
+bool overlap_add_frames_supported(const OlaArgs& a, const OlaFrameSet& fs, int bytes) {
+  if (fs.count < 1 || fs.count > kMaxGroupFrames) return false;
+  bool four = a.g.sx % 4 == 0 && a.g.ow % 4 == 0 && a.g.W % 4 == 0 && a.g.bw % 4 == 0;
+  for (int j = 0; j < fs.count && four; j++)
+    four = reinterpret_cast<uintptr_t>(fs.tdom[j]) % 16 == 0 &&
+           reinterpret_cast<uintptr_t>(fs.dst[j]) % (4 * bytes) == 0 && fs.dst_stride[j] % (4 * bytes) == 0;
+  return four;
+}
+
+cudaError_t launch_overlap_add_frames(const OlaArgs& a, const OlaFrameSet& fs, int bytes, cudaStream_t s) {
+  if (!overlap_add_frames_supported(a, fs, bytes)) return cudaErrorNotSupported;
+  dim3 block(kOlaTx, kOlaTy);
+  dim3 grid((a.g.W / 4 + kOlaTx - 1) / kOlaTx, (a.g.H + kOlaTy - 1) / kOlaTy, fs.count);
+  if (bytes == 1) k_overlap_add4_frames<uint8_t><<<grid, block, 0, s>>>(a, fs);
+  else if (bytes == 2) k_overlap_add4_frames<uint16_t><<<grid, block, 0, s>>>(a, fs);
+  else k_overlap_add4_frames<float><<<grid, block, 0, s>>>(a, fs);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_overlap_add(const OlaArgs& a, int bytes, cudaStream_t s) {

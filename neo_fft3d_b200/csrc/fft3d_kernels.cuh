@@ -115,6 +115,15 @@ struct FwdFrameSet {
   int ctas;
 };
 
+// The overlap-adds of a frame group in one launch: frame j's time-domain
+// blocks and destination plane (at the crop origin).
+struct OlaFrameSet {
+  const float* tdom[kMaxGroupFrames];
+  void* dst[kMaxGroupFrames];
+  long long dst_stride[kMaxGroupFrames];
+  int count;
+};
+
 // Forward transform of the window's newest frame fused with the filter and
 // the inverse transform (k_fused). f.src/f.spec: the newest frame and its ring
 // slot; v.in[]: the window's spectra (the newest frame's entry is f.spec).
@@ -164,6 +173,11 @@ cudaError_t launch_filter_inverse_frames(const InverseArgs& a, const FrameSet& f
 // what they share (geometry, windows, sample offset).
 cudaError_t launch_forward_frames(const ForwardArgs& a, const FwdFrameSet& fs, int bytes_per_sample, cudaStream_t s);
 cudaError_t launch_overlap_add(const OlaArgs& a, int bytes_per_sample, cudaStream_t s);
+// fs.count overlap-adds of one plane in one launch (a holds what they share);
+// cudaErrorNotSupported when a frame's geometry or alignment rules out the
+// 4-pixel kernel (then launch them one by one).
+cudaError_t launch_overlap_add_frames(const OlaArgs& a, const OlaFrameSet& fs, int bytes_per_sample, cudaStream_t s);
+bool overlap_add_frames_supported(const OlaArgs& a, const OlaFrameSet& fs, int bytes_per_sample);
 // Batched forms (work items as in BatchLaunch); OLA items are 32x8-pixel tiles.
 cudaError_t launch_forward_batch(int bw, int bh, const BatchLaunch& l, int bytes_per_sample, cudaStream_t s);
 cudaError_t launch_filter_inverse_batch(int bw, int bh, const BatchLaunch& l, int mode, cudaStream_t s);
