@@ -97,14 +97,17 @@ int fft3d_plane_filter_device(fft3d_plane* h, int n, const void* const src[5], c
  * j in [0, count + 4) with stride src_stride[j] (NULL outside the clip, or
  * where the frame's spectrum is cached); frame n0 + j is written to dst[j]
  * (stride dst_stride[j]); all work is queued on `stream` (NULL = the
- * handle's own stream). On the default path, Wiener 3D planes (bt = 2..5)
- * filter the group's frames with one filter/inverse launch whose CTAs
- * interleave the frames block range by block range, so that a window
- * spectrum shared by up to bt frames is read from HBM about once; the ring
- * keeps every spectrum the group needs and there is one time-domain buffer
- * per frame (both grow on first use: count + bt spectra and count - 1
- * buffers). Other planes filter the frames one after another. Outputs are
- * those of count calls of fft3d_plane_filter_device. */
+ * handle's own stream). On the default path, the group's new frames are
+ * transformed by one launch and its overlap-adds are one launch; Wiener 3D
+ * planes (bt = 2..5) filter the group's frames with one filter/inverse launch
+ * whose CTAs interleave the frames block range by block range, so that a
+ * window spectrum shared by up to bt frames is read from HBM about once
+ * (Kalman, Wiener 2D and sharpen-only planes: one filter/inverse launch per
+ * frame, in frame order). The ring keeps every spectrum the group needs and
+ * there is one time-domain buffer per frame (both grow on first use:
+ * count + bt spectra and count - 1 buffers). Planes on the other paths
+ * (tensor-core, fused, learned PSD) filter the frames one after another.
+ * Outputs are those of count calls of fft3d_plane_filter_device. */
 #define FFT3D_MAX_FRAME_GROUP 16
 int fft3d_plane_filter_frames_device(fft3d_plane* h, int n0, int count, const void* const* src,
                                      const int* src_stride, void* const* dst, const int* dst_stride, void* stream);
@@ -136,7 +139,9 @@ int fft3d_plane_geometry(fft3d_plane* h, int out[8]);
  * pattern-mode plane; a no-op otherwise. */
 int fft3d_plane_set_pattern_frame(fft3d_plane* h, const void* src, int src_stride);
 
-/* Drop all cached spectra and reset the Kalman state to its initial values. */
+/* Drop all cached spectra and reset the Kalman state to its initial values.
+ * Waits first for the work already queued for this plane, on whatever stream
+ * it was queued (device-buffer calls and batch steps included). */
 int fft3d_plane_reset(fft3d_plane* h);
 
 void fft3d_plane_destroy(fft3d_plane* h);

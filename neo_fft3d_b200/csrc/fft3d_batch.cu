@@ -511,6 +511,14 @@ int fft3d_batch_step(fft3d_batch* b, int count, fft3d_plane* const* planes, cons
   // the frames of a group share one CTA order, alternating from step to step
   const int reverse = (int)((uint64_t)b->stats[0] & 1);
   for (auto& kv : groups) kv.second.reverse = reverse;
+  // whatever the step queues on s, fft3d_plane_reset of its planes waits for it
+  struct MarkOnExit {
+    const std::vector<fft3d_plane*>& planes;
+    cudaStream_t s;
+    ~MarkOnExit() {
+      for (auto* P : planes) fft3d::plane_mark_work(P, s);
+    }
+  } mark_on_exit{order, s};
   for (int i = 0; i < count; i++) {
     d.plane = i;
     const fft3d::FrameGroup& g = groups[planes[i]];

@@ -45,6 +45,8 @@ int plane_bt(const fft3d_plane* P);
 // Forgets the spectra whose forward transforms d recorded for P (planning
 // failed, so they will not run).
 void plane_discard(fft3d_plane* P, const Deferred& d);
+// Records that P's work so far is queued on st (fft3d_plane_reset waits for it).
+void plane_mark_work(fft3d_plane* P, cudaStream_t st);
 std::mutex& plane_mutex(fft3d_plane* P);
 int plane_device(const fft3d_plane* P);
 // Empty when the scheduler can take the plane, else the reason.

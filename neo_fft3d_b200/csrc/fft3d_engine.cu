@@ -95,6 +95,14 @@ struct fft3d_plane {
   int keep_lo = 1, keep_hi = 0;
   int fixed_reverse = -1;
   uint64_t groups_done = 0;  // frame groups filtered (their CTA order alternates)
+  // completion of the last work queued for this plane on a caller's stream
+  // (device-buffer calls, batch steps): fft3d_plane_reset waits for it
+  // before it clears the ring and the Kalman state
+  cudaEvent_t last_work = nullptr;
+  // a reset queued on `stream` that the next call must wait for (on its own
+  // stream) before it reads the ring or the Kalman state
+  cudaEvent_t reset_done = nullptr;
+  bool reset_pending = false;
   float2* d_last = nullptr;
   float* d_cov = nullptr;
   float* d_covp = nullptr;
@@ -321,6 +329,11 @@ void free_plane(fft3d_plane* P) {
     if (gs.h_flags) cudaFreeHost(gs.h_flags);
   }
   for (auto e : P->sync_pool) cudaEventDestroy(e);
+  if (P->last_work) {
+    cudaEventSynchronize(P->last_work);
+    cudaEventDestroy(P->last_work);
+  }
+  if (P->reset_done) cudaEventDestroy(P->reset_done);
   if (P->s_up) cudaStreamDestroy(P->s_up);
   if (P->s_down) cudaStreamDestroy(P->s_down);
   if (P->stream) cudaStreamDestroy(P->stream);
@@ -461,6 +474,10 @@ int copy_plane(fft3d_plane* P, void* dst, int dstride, const void* src, int sstr
 
 int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride[5], void* dst, int dst_stride,
                bool host, cudaStream_t st) {
+  if (P->reset_pending) {  // fft3d_plane_reset queued on the plane's stream
+    CK(cudaStreamWaitEvent(st, P->reset_done, 0), "reset");
+    P->reset_pending = false;
+  }
   const fft3d_params& ep = P->ep;
   const int bt = ep.bt;
   int btcur = bt;  // src/fft3d_engine.h:579-582
@@ -826,6 +843,7 @@ int plane_plan(fft3d_plane* P, int n, const void* const src[5], const int stride
 
 int plane_bt(const fft3d_plane* P) { return P->ep.bt; }
 void plane_discard(fft3d_plane* P, const Deferred& d) { discard_recorded(P, d); }
+void plane_mark_work(fft3d_plane* P, cudaStream_t st);
 
 std::mutex& plane_mutex(fft3d_plane* P) { return P->mu; }
 int plane_device(const fft3d_plane* P) { return P->device; }
@@ -844,6 +862,16 @@ int engine_fail(int code, const std::string& msg) { return fail(code, msg); }
 
 namespace {
 
+// Records the completion of the work just queued for P on stream st.
+void mark_work(fft3d_plane* P, cudaStream_t st) {
+  if (!P->last_work && cudaEventCreateWithFlags(&P->last_work, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    P->last_work = nullptr;
+    return;
+  }
+  cudaEventRecord(P->last_work, st);
+}
+
 int check_group_args(const fft3d_plane* P, int count, const void* const* src, const int* src_stride,
                      void* const* dst, const int* dst_stride) {
   if (!P || !src || !src_stride || !dst || !dst_stride || count < 1 || count > FFT3D_MAX_FRAME_GROUP)
@@ -853,11 +881,13 @@ int check_group_args(const fft3d_plane* P, int count, const void* const* src, co
   return FFT3D_OK;
 }
 
-// Whether a call of `count` frames runs as a frame group: Wiener 3D planes on
-// the default path (Kalman state runs frame to frame; bt = 1 and sharpen-only
-// windows share no spectra).
+// Whether a call of `count` frames runs as a frame group: planes on the
+// default path. Their new frames' forward transforms and their overlap-adds
+// run as one launch each; the filter/inverse runs as one launch per run of
+// Wiener 3D frames and one launch per frame otherwise (Kalman, whose state
+// runs from frame to frame, in frame order).
 bool group_path(const fft3d_plane* P, int count) {
-  return count > 1 && P->ep.bt >= 2 && fft3d::plane_batchable(P).empty();
+  return count > 1 && fft3d::plane_batchable(P).empty();
 }
 
 // Frames n0 .. n0 + count - 1 from device frames (the window of frame n0 + j
@@ -1041,6 +1071,10 @@ int filter_group_host(fft3d_plane* P, int n0, int count, const void* const* src,
 }
 
 }  // namespace
+
+namespace fft3d {
+void plane_mark_work(fft3d_plane* P, cudaStream_t st) { mark_work(P, st); }
+}  // namespace fft3d
 
 extern "C" {
 
@@ -1268,15 +1302,20 @@ int fft3d_plane_reset(fft3d_plane* P) {
   if (!P) return fail(FFT3D_E_PARAM, "neo_fft3d: null handle");
   std::lock_guard<std::mutex> lk(P->mu);
   CK(cudaSetDevice(P->device), "cudaSetDevice");
+  // Stream-ordered: the reset runs on the plane's stream after the work
+  // already queued for the plane (on whatever stream), and the next call
+  // waits for it on its own stream; the host does not wait.
+  if (P->last_work) CK(cudaStreamWaitEvent(P->stream, P->last_work, 0), "reset");
   for (auto& s : P->slots) { s.frame = -1; s.stamp = 0; }
   if (P->ep.bt == 0) {
     const size_t n = P->spec_elems();
-    std::vector<float> init(n, P->sigma2n_2d);
     CK(cudaMemsetAsync(P->d_last, 0, n * sizeof(float2), P->stream), "Kalman reset");
-    CK(cudaMemcpyAsync(P->d_cov, init.data(), n * sizeof(float), cudaMemcpyHostToDevice, P->stream), "Kalman reset");
-    CK(cudaMemcpyAsync(P->d_covp, init.data(), n * sizeof(float), cudaMemcpyHostToDevice, P->stream), "Kalman reset");
-    CK(cudaStreamSynchronize(P->stream), "Kalman reset");
+    CK(fft3d::launch_fill(P->d_cov, P->sigma2n_2d, n, P->stream), "Kalman reset");
+    CK(fft3d::launch_fill(P->d_covp, P->sigma2n_2d, n, P->stream), "Kalman reset");
   }
+  if (!P->reset_done) CK(cudaEventCreateWithFlags(&P->reset_done, cudaEventDisableTiming), "reset");
+  CK(cudaEventRecord(P->reset_done, P->stream), "reset");
+  P->reset_pending = true;
   return FFT3D_OK;
 }
 
@@ -1318,7 +1357,10 @@ int fft3d_plane_filter_device(fft3d_plane* P, int n, const void* const src[5], c
   if (!P || !dst) return fail(FFT3D_E_PARAM, "neo_fft3d: null argument");
   std::lock_guard<std::mutex> lk(P->mu);
   CK(cudaSetDevice(P->device), "cudaSetDevice");
-  return run_filter(P, n, src, src_stride, dst, dst_stride, false, stream ? (cudaStream_t)stream : P->stream);
+  cudaStream_t st = stream ? (cudaStream_t)stream : P->stream;
+  const int rc = run_filter(P, n, src, src_stride, dst, dst_stride, false, st);
+  mark_work(P, st);
+  return rc;
 }
 
 int fft3d_plane_filter_frames_device(fft3d_plane* P, int n0, int count, const void* const* src, const int* src_stride,
@@ -1327,7 +1369,10 @@ int fft3d_plane_filter_frames_device(fft3d_plane* P, int n0, int count, const vo
   if (rc) return rc;
   std::lock_guard<std::mutex> lk(P->mu);
   CK(cudaSetDevice(P->device), "cudaSetDevice");
-  return filter_group(P, n0, count, src, src_stride, dst, dst_stride, stream ? (cudaStream_t)stream : P->stream);
+  cudaStream_t st = stream ? (cudaStream_t)stream : P->stream;
+  rc = filter_group(P, n0, count, src, src_stride, dst, dst_stride, st);
+  mark_work(P, st);
+  return rc;
 }
 
 int fft3d_plane_filter_frames(fft3d_plane* P, int n0, int count, const void* const* src, const int* src_stride,

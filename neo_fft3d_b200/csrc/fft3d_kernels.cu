@@ -393,6 +393,17 @@ bool overlap_add_frames_supported(const OlaArgs& a, const OlaFrameSet& fs, int b
   return four;
 }
 
+__global__ void k_fill(float* p, float v, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
+}
+
+cudaError_t launch_fill(float* p, float v, size_t n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const int grid = (int)std::min<size_t>((n + 255) / 256, 4096);
+  k_fill<<<grid, 256, 0, s>>>(p, v, n);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_overlap_add_frames(const OlaArgs& a, const OlaFrameSet& fs, int bytes, cudaStream_t s) {
   if (!overlap_add_frames_supported(a, fs, bytes)) return cudaErrorNotSupported;
   dim3 block(kOlaTx, kOlaTy);

@@ -173,6 +173,8 @@ cudaError_t launch_filter_inverse_frames(const InverseArgs& a, const FrameSet& f
 // what they share (geometry, windows, sample offset).
 cudaError_t launch_forward_frames(const ForwardArgs& a, const FwdFrameSet& fs, int bytes_per_sample, cudaStream_t s);
 cudaError_t launch_overlap_add(const OlaArgs& a, int bytes_per_sample, cudaStream_t s);
+// p[0 .. n) = v (stream-ordered state resets)
+cudaError_t launch_fill(float* p, float v, size_t n, cudaStream_t s);
 // fs.count overlap-adds of one plane in one launch (a holds what they share);
 // cudaErrorNotSupported when a frame's geometry or alignment rules out the
 // 4-pixel kernel (then launch them one by one).

@@ -231,3 +231,36 @@ def test_host_frame_groups_from_threads(gpu):
         assert np.array_equal(r, g)
     for e in engs:
         e.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("grouped", [False, True], ids=["one_frame_per_call", "frame_groups"])
+def test_reset_waits_for_queued_work(gpu, grouped):
+    """fft3d_plane_reset right after frames were queued on a caller's stream
+    (no host synchronisation) must not clear the Kalman state under those
+    frames' kernels: every pass over the clip gives the same output."""
+    import torch
+    clip = dict(width=640, height=480, bits=8, seed=91)
+    planes, dev = _clip(torch, clip)
+    a = dev[0]
+    p = make_params(sigma=3.0, bt=0)
+    e = engine.PlaneEngine(p, plane_descs([a.shape[1:]], 8, F)[0])
+    s = torch.cuda.Stream()
+    st = a.shape[2]
+    outs = []
+    for _ in range(3):
+        o = torch.empty_like(a)
+        e.reset()
+        if grouped:
+            for n0 in range(0, F, 8):
+                k = min(8, F - n0)
+                e.filter_frames_device(n0, [_ptr(a, n) for n in range(n0 - 2, n0 + k + 2)], [st] * (k + 4),
+                                       [_ptr(o, n) for n in range(n0, n0 + k)], [st] * k, s.cuda_stream)
+        else:
+            for n in range(F):
+                e.filter_device(n, [0, 0, _ptr(a, n), 0, 0], [st] * 5, _ptr(o, n), st, s.cuda_stream)
+        outs.append(o)
+    torch.cuda.synchronize()
+    for o in outs[1:]:
+        assert torch.equal(outs[0], o)
+    e.close()
