@@ -54,8 +54,10 @@ METRIC = "1080p bt=5 frames/s: TC split-precision vs plain FP32 kernel at \u00b1
 UNIT = "frames/s"
 # the two forms of the block transform that the metric compares (NEO_FFT3D_PATH)
 PATHS = {"plain_fp32": "unfused", "plain_fp32_fused": "fused", "plain_fp32_frames": "unfused",
-         "tc_split_bf16": "tc"}
+         "tc_split_bf16": "tc", "tc_split_bf16_frames": "tc"}
 PLAIN = ("plain_fp32", "plain_fp32_fused", "plain_fp32_frames")
+TC = ("tc_split_bf16", "tc_split_bf16_frames")
+GROUPED = ("plain_fp32_frames", "tc_split_bf16_frames")
 # output frames per call of the grouped arm (fft3d_plane_filter_frames_device)
 FRAME_GROUP = 8
 
@@ -367,7 +369,7 @@ def main():
     for a in chosen:
         if a not in PATHS:
             raise SystemExit(f"unknown arm {a}; arms: {', '.join(PATHS)}")
-    arms = {name: make_arm(path, FRAME_GROUP if name == "plain_fp32_frames" else 0)
+    arms = {name: make_arm(path, FRAME_GROUP if name in GROUPED else 0)
             for name, path in PATHS.items() if name in chosen}
     os.environ["NEO_FFT3D_PATH"] = PATHS["plain_fp32"]
     clocks = ClockSampler(local)
@@ -393,7 +395,11 @@ def main():
             within += int((d <= 1).sum().item())
             total_px += d.numel()
         best_plain = max(arms[k]["value"] for k in PLAIN)
-        paths["tc_over_plain"] = arms["tc_split_bf16"]["value"] / best_plain
+        paths["tc_over_plain"] = max(arms[k]["value"] for k in TC) / best_plain
+        # the same schedule (frame groups of FRAME_GROUP) for both transforms
+        paths["tc_frames_over_plain_frames"] = arms["tc_split_bf16_frames"]["value"] / arms["plain_fp32_frames"]["value"]
+        paths["tc_frames_vs_tc_output_identical"] = all(
+            bool(torch.equal(a, b)) for a, b in zip(arms["tc_split_bf16"]["outs"], arms["tc_split_bf16_frames"]["outs"]))
         # the fused sequence against the unfused one (same FP32 arithmetic)
         fd_max, fd_within = 0, 0
         for a, b in zip(arms["plain_fp32"]["outs"], arms["plain_fp32_fused"]["outs"]):

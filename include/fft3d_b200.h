@@ -97,8 +97,9 @@ int fft3d_plane_filter_device(fft3d_plane* h, int n, const void* const src[5], c
  * j in [0, count + 4) with stride src_stride[j] (NULL outside the clip, or
  * where the frame's spectrum is cached); frame n0 + j is written to dst[j]
  * (stride dst_stride[j]); all work is queued on `stream` (NULL = the
- * handle's own stream). On the default path, the group's new frames are
- * transformed by one launch and its overlap-adds are one launch; Wiener 3D
+ * handle's own stream). On the default and tensor-core paths, the group's
+ * new frames are transformed by one launch (tensor-core: one per frame) and
+ * its overlap-adds are one launch; Wiener 3D
  * planes (bt = 2..5) filter the group's frames with one filter/inverse launch
  * whose CTAs interleave the frames block range by block range, so that a
  * window spectrum shared by up to bt frames is read from HBM about once
@@ -106,7 +107,7 @@ int fft3d_plane_filter_device(fft3d_plane* h, int n, const void* const src[5], c
  * frame, in frame order). The ring keeps every spectrum the group needs and
  * there is one time-domain buffer per frame (both grow on first use:
  * count + bt spectra and count - 1 buffers). Planes on the other paths
- * (tensor-core, fused, learned PSD) filter the frames one after another.
+ * (fused, learned PSD, bulk-staged) filter the frames one after another.
  * Outputs are those of count calls of fft3d_plane_filter_device. */
 #define FFT3D_MAX_FRAME_GROUP 16
 int fft3d_plane_filter_frames_device(fft3d_plane* h, int n0, int count, const void* const* src,

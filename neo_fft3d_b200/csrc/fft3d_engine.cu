@@ -724,8 +724,16 @@ int run_group(fft3d_plane* P, const fft3d::Deferred& d, cudaStream_t st) {
   const double S = (double)P->spec_elems() * sizeof(float2);
   const double T = (double)P->g.nblocks * P->g.bh * P->g.bw * 4;
   const double pix = (double)P->g.W * P->g.H * P->bytes;
-  // the new frames' forward transforms: one launch for all of them
-  for (size_t i = 0; i < d.fwd.size();) {
+  // the new frames' forward transforms: one launch for all of them (the
+  // tensor-core transform: one launch per frame)
+  if (P->d_tc) {
+    for (const auto& f : d.fwd) {
+      TimeScope ts(P, K_FORWARD, pix + S, st);
+      CK(fft3d::launch_forward_tc(f.a, P->d_tc, P->d_err, f.bytes, st), "tensor-core forward kernel");
+      g_launches++;
+    }
+  }
+  for (size_t i = 0; i < (P->d_tc ? 0 : d.fwd.size());) {
     const size_t e = std::min(d.fwd.size(), i + (size_t)fft3d::kMaxFwdFrames);
     TimeScope ts(P, K_FORWARD, (double)(e - i) * (pix + S), st);
     if (e - i == 1) {
@@ -882,12 +890,13 @@ int check_group_args(const fft3d_plane* P, int count, const void* const* src, co
 }
 
 // Whether a call of `count` frames runs as a frame group: planes on the
-// default path. Their new frames' forward transforms and their overlap-adds
-// run as one launch each; the filter/inverse runs as one launch per run of
+// default or the tensor-core path. Their new frames' forward transforms
+// (tensor-core: one launch per frame) and their overlap-adds run as one
+// launch each; the filter/inverse runs as one launch per run of
 // Wiener 3D frames and one launch per frame otherwise (Kalman, whose state
 // runs from frame to frame, in frame order).
 bool group_path(const fft3d_plane* P, int count) {
-  return count > 1 && fft3d::plane_batchable(P).empty();
+  return count > 1 && (P->path == 1 || P->path == 3) && !P->psd_model && !P->bulk;
 }
 
 // Frames n0 .. n0 + count - 1 from device frames (the window of frame n0 + j

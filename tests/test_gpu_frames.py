@@ -96,15 +96,18 @@ def test_frame_groups_match_per_frame(gpu, name, clip, filt):
 
 @pytest.mark.gpu
 def test_frame_groups_tensor_core_path(gpu, monkeypatch):
-    """The tensor-core path takes frame groups one frame at a time."""
+    """The tensor-core path in frame groups (its forward transform per frame,
+    the grouped filter/inverse and overlap-add) equals it one frame at a
+    time."""
     import torch
     monkeypatch.setenv("NEO_FFT3D_PATH", "tc")
     clip, filt = CASES[0][1], CASES[0][2]
     planes, dev = _clip(torch, clip)
     ref = _per_frame(torch, planes, dev, clip, filt)
-    got = _grouped(torch, planes, dev, clip, filt, [5])
-    for r, g in zip(ref, got):
-        assert np.array_equal(r, g)
+    for sizes in ([5], [8, 3]):
+        got = _grouped(torch, planes, dev, clip, filt, sizes)
+        for r, g in zip(ref, got):
+            assert np.array_equal(r, g)
 
 
 @pytest.mark.gpu
