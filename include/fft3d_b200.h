@@ -98,8 +98,8 @@ int fft3d_plane_filter_device(fft3d_plane* h, int n, const void* const src[5], c
  * where the frame's spectrum is cached); frame n0 + j is written to dst[j]
  * (stride dst_stride[j]); all work is queued on `stream` (NULL = the
  * handle's own stream). On the default and tensor-core paths, the group's
- * new frames are transformed by one launch (tensor-core: one per frame) and
- * its overlap-adds are one launch; Wiener 3D
+ * new frames are transformed by one launch and its overlap-adds are one
+ * launch; Wiener 3D
  * planes (bt = 2..5) filter the group's frames with one filter/inverse launch
  * whose CTAs interleave the frames block range by block range, so that a
  * window spectrum shared by up to bt frames is read from HBM about once

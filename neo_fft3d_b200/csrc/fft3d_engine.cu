@@ -724,28 +724,23 @@ int run_group(fft3d_plane* P, const fft3d::Deferred& d, cudaStream_t st) {
   const double S = (double)P->spec_elems() * sizeof(float2);
   const double T = (double)P->g.nblocks * P->g.bh * P->g.bw * 4;
   const double pix = (double)P->g.W * P->g.H * P->bytes;
-  // the new frames' forward transforms: one launch for all of them (the
-  // tensor-core transform: one launch per frame)
-  if (P->d_tc) {
-    for (const auto& f : d.fwd) {
-      TimeScope ts(P, K_FORWARD, pix + S, st);
-      CK(fft3d::launch_forward_tc(f.a, P->d_tc, P->d_err, f.bytes, st), "tensor-core forward kernel");
-      g_launches++;
-    }
-  }
-  for (size_t i = 0; i < (P->d_tc ? 0 : d.fwd.size());) {
+  // the new frames' forward transforms: one launch for all of them
+  for (size_t i = 0; i < d.fwd.size();) {
     const size_t e = std::min(d.fwd.size(), i + (size_t)fft3d::kMaxFwdFrames);
     TimeScope ts(P, K_FORWARD, (double)(e - i) * (pix + S), st);
-    if (e - i == 1) {
+    fft3d::FwdFrameSet fs{};
+    fs.count = (int)(e - i);
+    for (size_t k = i; k < e; k++) {
+      fs.src[k - i] = d.fwd[k].a.src;
+      fs.stride[k - i] = d.fwd[k].a.src_stride;
+      fs.spec[k - i] = d.fwd[k].a.spec;
+    }
+    if (P->d_tc) {
+      CK(fft3d::launch_forward_tc_frames(d.fwd[i].a, fs, P->d_tc, P->d_err, d.fwd[i].bytes, st),
+         "tensor-core forward kernel (frame group)");
+    } else if (e - i == 1) {
       CK(fft3d::launch_forward(d.fwd[i].a, d.fwd[i].bytes, st), "forward kernel");
     } else {
-      fft3d::FwdFrameSet fs{};
-      fs.count = (int)(e - i);
-      for (size_t k = i; k < e; k++) {
-        fs.src[k - i] = d.fwd[k].a.src;
-        fs.stride[k - i] = d.fwd[k].a.src_stride;
-        fs.spec[k - i] = d.fwd[k].a.spec;
-      }
       CK(fft3d::launch_forward_frames(d.fwd[i].a, fs, d.fwd[i].bytes, st), "forward kernel (frame group)");
     }
     g_launches++;
@@ -890,9 +885,9 @@ int check_group_args(const fft3d_plane* P, int count, const void* const* src, co
 }
 
 // Whether a call of `count` frames runs as a frame group: planes on the
-// default or the tensor-core path. Their new frames' forward transforms
-// (tensor-core: one launch per frame) and their overlap-adds run as one
-// launch each; the filter/inverse runs as one launch per run of
+// default or the tensor-core path. Their new frames' forward transforms and
+// their overlap-adds run as one launch each; the filter/inverse runs as one
+// launch per run of
 // Wiener 3D frames and one launch per frame otherwise (Kalman, whose state
 // runs from frame to frame, in frame order).
 bool group_path(const fft3d_plane* P, int count) {

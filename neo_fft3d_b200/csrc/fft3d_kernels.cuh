@@ -210,6 +210,10 @@ uint32_t forward_tc_table_bytes();
 uint32_t forward_tc_smem_bytes();
 void forward_tc_tables(const float* wx, const float* wy, uint8_t* out);
 cudaError_t launch_forward_tc(const ForwardArgs& a, const void* tables, int* err, int bytes_per_sample, cudaStream_t s);
+// The tensor-core forward transforms of fs.count frames of one plane in one
+// persistent launch (work items: the frames' tiles).
+cudaError_t launch_forward_tc_frames(const ForwardArgs& a, const FwdFrameSet& fs, const void* tables, int* err,
+                                     int bytes_per_sample, cudaStream_t s);
 
 // Sets the message returned by fft3d_last_error() on this thread.
 void set_last_error(const std::string& msg);

@@ -145,7 +145,7 @@ constexpr uint32_t SMEM_TC_SPLIT = OFF_A1L + 2 * SZ_A1;    // V split (9..16-bit
 constexpr uint32_t TABLE_BYTES = 2 * SZ_B1 + 2 * SZ_B2;    // global image of B1h, B1l, B2h, B2l
 
 template <typename T, bool VSPLIT>
-__global__ void __launch_bounds__(THREADS) k_forward_tc(ForwardArgs a, const uint8_t* __restrict__ tables,
+__global__ void __launch_bounds__(THREADS) k_forward_tc(ForwardArgs a, FwdFrameSet fs, const uint8_t* __restrict__ tables,
                                                         int* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t sm[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + OFF_BAR);
@@ -174,41 +174,91 @@ __global__ void __launch_bounds__(THREADS) k_forward_tc(ForwardArgs a, const uin
   const uint32_t d1 = tmem;       // stage 1: sub-tile s at columns 32 s
   const uint32_t d2 = tmem + 64;  // stage 2: 64 columns
   const uint32_t sbase = smem_u32(sm);
+  // work item t: tile t % ntiles of frame t / ntiles (fs: the frames' samples
+  // and ring slots)
   const int ntiles = (g.nblocks + TILE - 1) / TILE;
+  const int total = ntiles * fs.count;
+  auto frame_of = [&](int t, const void** src, long long* stride, float2** spec) {
+    const int j = t / ntiles;
+#pragma unroll
+    for (int q = 0; q < kMaxFwdFrames; q++)
+      if (q == j) {
+        *src = fs.src[q];
+        *stride = fs.stride[q];
+        *spec = fs.spec[q];
+      }
+  };
+  // Rows of a tile: thread tid holds rows tid and tid + 128 of the tile's 256
+  // (8 blocks x 32 rows). Interior aligned rows of 8- and 16-bit samples are
+  // fetched as raw 16-byte vectors one tile ahead, so their load latency
+  // overlaps the previous tile's MMAs.
+  constexpr int RPT = ROWS / THREADS;
+  constexpr int NV = sizeof(T) <= 2 ? TB * (int)sizeof(T) / 16 : 0;
+  uint4 raw[RPT][NV > 0 ? NV : 1];
+  bool have[RPT];
+  auto row_src = [&](const void* src, long long stride, int blk, int y, int* x0) {
+    const int by = blk / g.nox, bx = blk - by * g.nox;
+    const int kr = reflect101_tc(by * g.sy + y - g.sy, g.H);
+    const int row = g.interlaced ? (kr < (g.H >> 1) ? 2 * kr : g.H - 1 - 2 * (kr - (g.H >> 1))) : kr;
+    *x0 = bx * g.sx - g.sx;
+    return reinterpret_cast<const T*>(static_cast<const char*>(src) + (long long)row * stride);
+  };
+  auto prefetch = [&](int t) {
+#pragma unroll
+    for (int i = 0; i < RPT; i++) have[i] = false;
+    if constexpr (NV > 0) {
+      if (t >= total) return;
+      const void* src;
+      long long stride;
+      float2* spec;
+      frame_of(t, &src, &stride, &spec);
+      const int blk0 = (t % ntiles) * TILE;
+#pragma unroll
+      for (int i = 0; i < RPT; i++) {
+        const int r = tid + THREADS * i, b = r / TB, y = r - b * TB, blk = blk0 + b;
+        if (blk < g.nblocks) {
+          int x0;
+          const T* p = row_src(src, stride, blk, y, &x0) + x0;
+          if (x0 >= 0 && x0 + TB <= g.W && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+#pragma unroll
+            for (int v = 0; v < NV; v++) raw[i][v] = __ldg(reinterpret_cast<const uint4*>(p) + v);
+            have[i] = true;
+          }
+        }
+      }
+    }
+  };
   uint32_t phase = 0;
   bool ok = true;
-  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    const int blk0 = tile * TILE;
+  prefetch(blockIdx.x);
+  for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+    const void* fsrc;
+    long long fstride;
+    float2* fspec;
+    frame_of(t, &fsrc, &fstride, &fspec);
+    const int blk0 = (t % ntiles) * TILE;
     // ---- stage 1 operand: rows of V (two rows per thread)
-    for (int r = tid; r < ROWS; r += THREADS) {
+#pragma unroll
+    for (int i = 0; i < RPT; i++) {
+      const int r = tid + THREADS * i;
       const int b = r / TB, y = r - b * TB, blk = blk0 + b;
       const int sub = r >> 7, m = r & 127;
       uint8_t* ah = sm + OFF_A1H + sub * SZ_A1;
       uint8_t* al = sm + OFF_A1L + sub * SZ_A1;
       float v[TB];
       if (blk < g.nblocks) {
-        const int by = blk / g.nox, bx = blk - by * g.nox;
-        const int kr = reflect101_tc(by * g.sy + y - g.sy, g.H);
-        const int row = g.interlaced ? (kr < (g.H >> 1) ? 2 * kr : g.H - 1 - 2 * (kr - (g.H >> 1))) : kr;
-        const T* srow = reinterpret_cast<const T*>(static_cast<const char*>(a.src) + (long long)row * a.src_stride);
-        const int x0 = bx * g.sx - g.sx;
-        const float wy = 1.f;  // the y window is folded into stage 2
-        (void)wy;
-        const T* p = srow + x0;
-        if (x0 >= 0 && x0 + TB <= g.W && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
-          // 16-byte loads of the row (the common interior case)
+        int x0;
+        const T* srow = row_src(fsrc, fstride, blk, y, &x0);
+        if (NV > 0 && have[i]) {
           constexpr int PER = 16 / (int)sizeof(T);
-          const uint4* q = reinterpret_cast<const uint4*>(p);
 #pragma unroll
-          for (int c = 0; c < TB / PER; c++) {
-            const uint4 u = __ldg(q + c);
-            const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+          for (int c = 0; c < (NV > 0 ? NV : 1); c++) {
+            const uint32_t w[4] = {raw[i][c].x, raw[i][c].y, raw[i][c].z, raw[i][c].w};
 #pragma unroll
             for (int j = 0; j < PER; j++) {
               float f;
               if constexpr (sizeof(T) == 1) f = (float)((w[j >> 2] >> (8 * (j & 3))) & 0xffu);
-              else if constexpr (sizeof(T) == 2) f = (float)((w[j >> 1] >> (16 * (j & 1))) & 0xffffu);
-              else f = __uint_as_float(w[j]);
+              else f = (float)((w[j >> 1] >> (16 * (j & 1))) & 0xffffu);
               v[c * PER + j] = f - a.base;
             }
           }
@@ -253,6 +303,7 @@ __global__ void __launch_bounds__(THREADS) k_forward_tc(ForwardArgs a, const uin
       }
       mma_commit(bar);
     }
+    prefetch(t + gridDim.x);  // the next tile's rows load while this tile's MMAs run
     if (__syncthreads_or(mbar_wait(bar, phase) ? 0 : 1)) {  // uniform verdict: no thread left at a barrier
       ok = false;
       if (tid == 0) atomicOr(err, 1);
@@ -332,7 +383,7 @@ __global__ void __launch_bounds__(THREADS) k_forward_tc(ForwardArgs a, const uin
     {
       const int nvalid = min(TILE, g.nblocks - blk0);
       const uint4* src = reinterpret_cast<const uint4*>(stage);
-      uint4* dst = reinterpret_cast<uint4*>(a.spec + (size_t)blk0 * TB * NH);
+      uint4* dst = reinterpret_cast<uint4*>(fspec + (size_t)blk0 * TB * NH);
       for (int i = tid; i < nvalid * TB * NH / 2; i += THREADS) dst[i] = src[i];
     }
     tc_fence_before();
@@ -387,24 +438,34 @@ void forward_tc_tables(const float* wx, const float* wy, uint8_t* out) {
 }
 
 cudaError_t launch_forward_tc(const ForwardArgs& a, const void* tables, int* err, int bytes, cudaStream_t s) {
-  if (a.g.bw != TB || a.g.bh != TB) return cudaErrorInvalidValue;
+  FwdFrameSet fs{};
+  fs.count = 1;
+  fs.src[0] = a.src;
+  fs.stride[0] = a.src_stride;
+  fs.spec[0] = a.spec;
+  return launch_forward_tc_frames(a, fs, tables, err, bytes, s);
+}
+
+cudaError_t launch_forward_tc_frames(const ForwardArgs& a, const FwdFrameSet& fs, const void* tables, int* err,
+                                     int bytes, cudaStream_t s) {
+  if (a.g.bw != TB || a.g.bh != TB || fs.count < 1 || fs.count > kMaxFwdFrames) return cudaErrorInvalidValue;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int ntiles = (a.g.nblocks + TILE - 1) / TILE;
+  const int ntiles = (a.g.nblocks + TILE - 1) / TILE * fs.count;
   const int per_sm = bytes == 1 ? 3 : 2;  // shared memory limits co-resident CTAs
   const int grid = ntiles < sms * per_sm ? ntiles : sms * per_sm;
   const uint8_t* t = static_cast<const uint8_t*>(tables);
   cudaError_t e = cudaSuccess;
   if (bytes == 1) {
     e = fft3d::smem_attr(k_forward_tc<uint8_t, false>, SMEM_TC, true);
-    if (e == cudaSuccess) k_forward_tc<uint8_t, false><<<grid, THREADS, SMEM_TC, s>>>(a, t, err);
+    if (e == cudaSuccess) k_forward_tc<uint8_t, false><<<grid, THREADS, SMEM_TC, s>>>(a, fs, t, err);
   } else if (bytes == 2) {
     e = fft3d::smem_attr(k_forward_tc<uint16_t, true>, SMEM_TC_SPLIT, true);
-    if (e == cudaSuccess) k_forward_tc<uint16_t, true><<<grid, THREADS, SMEM_TC_SPLIT, s>>>(a, t, err);
+    if (e == cudaSuccess) k_forward_tc<uint16_t, true><<<grid, THREADS, SMEM_TC_SPLIT, s>>>(a, fs, t, err);
   } else {
     e = fft3d::smem_attr(k_forward_tc<float, true>, SMEM_TC_SPLIT, true);
-    if (e == cudaSuccess) k_forward_tc<float, true><<<grid, THREADS, SMEM_TC_SPLIT, s>>>(a, t, err);
+    if (e == cudaSuccess) k_forward_tc<float, true><<<grid, THREADS, SMEM_TC_SPLIT, s>>>(a, fs, t, err);
   }
   return e != cudaSuccess ? e : cudaGetLastError();
 }
