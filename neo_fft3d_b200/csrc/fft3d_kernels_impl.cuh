@@ -593,6 +593,14 @@ __host__ __device__ constexpr int fft_ctas(int nblocks) {
   return (nblocks + kWarps * blocks_per_warp<BW>() - 1) / (kWarps * blocks_per_warp<BW>());
 }
 
+// A window-spectrum value, read once per CTA: not kept in L1, where the
+// per-bin tables (grid, wsharpen) that every chunk reads should stay.
+__device__ __forceinline__ float2 ld_stream(const float2* p) {
+  float2 v;
+  asm("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+  return v;
+}
+
 // Where a CTA finds its window spectra and writes its time-domain blocks:
 // the launch arguments (one output frame per launch), or pointers picked for
 // one frame of a frame group (k_filter_inverse_frames).
@@ -649,7 +657,7 @@ __device__ __forceinline__ void filter_inverse_cta_w(const InverseArgs& a, int v
     auto load = [&](int j, float2(&dst)[NGB]) {
       const int i = lane + 32 * j;
 #pragma unroll
-      for (int k = 0; k < NG; k++) dst[k] = i < BINS ? __ldg(win.in(LO + k) + off + i) : make_float2(0.f, 0.f);
+      for (int k = 0; k < NG; k++) dst[k] = i < BINS ? ld_stream(win.in(LO + k) + off + i) : make_float2(0.f, 0.f);
     };
     if constexpr (NG > 0) {
 #pragma unroll
