@@ -135,8 +135,14 @@ __device__ __forceinline__ void overlap_add_px4(const OlaArgs& a, int x0, int k)
   const int bx = X / g.sx, x = X - bx * g.sx;
   const bool yov = y < g.oh, xov = x < g.ow;
   const int bw = g.bw, bh = g.bh;
+  // time-domain values are read once: not kept in L1, where the synthesis
+  // windows stay
   auto at4 = [&](int bxx, int byy, int yy, int xx) {
-    const float4 q = __ldg(reinterpret_cast<const float4*>(a.tdom + ((size_t)(byy * g.nox + bxx) * bh + yy) * bw + xx));
+    const float* p = a.tdom + ((size_t)(byy * g.nox + bxx) * bh + yy) * bw + xx;
+    float4 q;
+    asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+        : "=f"(q.x), "=f"(q.y), "=f"(q.z), "=f"(q.w)
+        : "l"(p));
     return q;
   };
   auto comp = [](const float4& q, int i) { return i == 0 ? q.x : (i == 1 ? q.y : (i == 2 ? q.z : q.w)); };
