@@ -81,6 +81,7 @@ struct fft3d_plane {
   fft3d::Tables tab{};
   const float* d_wan_x = nullptr;
   const float* d_wan_y = nullptr;
+  std::vector<float> h_wan_x;  // host copy of the analysis window along x
   float* d_pattern2d = nullptr;
   float* d_pattern3d = nullptr;
   std::vector<Slot> slots;
@@ -374,6 +375,7 @@ fft3d::ForwardArgs forward_args(fft3d_plane* P, const void* plane, long long str
   a.base = (P->bytes != 4 && P->d.is_chroma) ? (float)(1 << (P->d.bits - 1)) : 0.f;
   a.wan_x = P->d_wan_x;
   a.wan_y = P->d_wan_y;
+  for (int x = 0; x < fft3d::kMaxBw; x++) a.wx[x] = x < (int)P->h_wan_x.size() ? P->h_wan_x[x] : 0.f;
   a.spec = spec;
   return a;
 }
@@ -1158,6 +1160,7 @@ int fft3d_plane_create(const fft3d_params* p, const fft3d_plane_desc* d, int dev
   windows(ep, ep.ow, axl, axr, sxl, sxr);
   windows(ep, ep.oh, ayl, ayr, syl, syr);
   std::vector<float> wx = full_window(ep.bw, ep.ow, axl, axr), wy = full_window(ep.bh, ep.oh, ayl, ayr);
+  P->h_wan_x = wx;
   const int bh = ep.bh, bw = ep.bw, nh = g.nh, nb = bh * nh;
   std::vector<float> wsharpen(nb), wdehalo(nb);
   float wmax = 0;

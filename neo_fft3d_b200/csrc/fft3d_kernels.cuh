@@ -64,6 +64,7 @@ struct FilterConsts {
   int use_sharpen, use_dehalo;
 };
 
+constexpr int kMaxBw = 64;  // largest block width the kernels are built for (48) rounded up
 struct ForwardArgs {
   Geom g;
   const void* src;        // frame plane at the crop origin
@@ -72,6 +73,8 @@ struct ForwardArgs {
   const float* wan_x;
   const float* wan_y;
   float2* spec;           // blocks x bh x nh
+  float wx[kMaxBw];       // wan_x by value: read through the launch parameters
+                          // (constant-bank operands) by the per-plane kernels
 };
 
 struct InverseArgs {

@@ -143,7 +143,7 @@ __device__ __forceinline__ void decode_row(const uint4* raw, float (&r)[BW]) {
 // Row y of block `blk`: gather (mirrored at the plane edges), analysis window,
 // r2c along x into row y of Sb. `raw`: the row's samples already fetched
 // (interior aligned rows), or null.
-template <int BW, int BH, typename T, class Win>
+template <int BW, int BH, typename T, bool ARGS_WX, class Win>
 __device__ __forceinline__ void fwd_row(const ForwardArgs& a, const Win& win, int blk, int y, float2* Sb,
                                         const uint4* raw) {
   constexpr int NH = BW / 2 + 1;
@@ -162,8 +162,9 @@ __device__ __forceinline__ void fwd_row(const ForwardArgs& a, const Win& win, in
     for (int x = 0; x < BW; x++) r[x] = load_sample<T>(srow + reflect101(x0 + x, g.W));
   }
   const float wy = __ldg(a.wan_y + y);
+  // the x window from the launch parameters (ARGS_WX) or from the table
 #pragma unroll
-  for (int x = 0; x < BW; x++) r[x] = (r[x] - a.base) * __ldg(a.wan_x + x) * wy;
+  for (int x = 0; x < BW; x++) r[x] = (r[x] - a.base) * (ARGS_WX ? a.wx[x] : __ldg(a.wan_x + x)) * wy;
   float2 c[NH];
   rfft<BW>(r, c);
   float2* row = Sb + y * NH;
@@ -256,8 +257,10 @@ __device__ __forceinline__ void store_tdom(const float2* Sb, float* out, int lan
 
 // One warp transforms blocks_per_warp<BW>() consecutive blocks (rows, then
 // columns, then a coalesced 16-byte copy-out of the contiguous spectra).
-// PREFETCH: fetch every row of the lane before the first transform (more
-// registers; off where the kernel's register budget is tight).
+// PREFETCH: fetch every row of the lane before the first transform, and take
+// the x window from the launch parameters (more registers and a parameter-
+// space ForwardArgs; off where the register budget is tight or the arguments
+// are a copy in registers).
 template <int BW, int BH, typename T, bool PREFETCH, class Win>
 __device__ __forceinline__ void forward_cta_w(const ForwardArgs& a, int cta, const Win& win) {
   constexpr int NH = BW / 2 + 1, HC = BW / 2, NBW = blocks_per_warp<BW>(), BINS = BH * NH;
@@ -293,12 +296,12 @@ __device__ __forceinline__ void forward_cta_w(const ForwardArgs& a, int cta, con
     for (int i = 0; i < RPL; i++) {
       const int t = lane + 32 * i, b = t / BH, y = t - b * BH;
       if (t < NBW * BH && blk0 + b < g.nblocks)
-        fwd_row<BW, BH, T>(a, win, blk0 + b, y, S + b * BINS, have[i] ? raw[i] : nullptr);
+        fwd_row<BW, BH, T, PREFETCH>(a, win, blk0 + b, y, S + b * BINS, have[i] ? raw[i] : nullptr);
     }
   } else {
     for (int t = lane; t < NBW * BH; t += 32) {
       const int b = t / BH, y = t - b * BH;
-      if (blk0 + b < g.nblocks) fwd_row<BW, BH, T>(a, win, blk0 + b, y, S + b * BINS, nullptr);
+      if (blk0 + b < g.nblocks) fwd_row<BW, BH, T, PREFETCH>(a, win, blk0 + b, y, S + b * BINS, nullptr);
     }
   }
   __syncwarp();

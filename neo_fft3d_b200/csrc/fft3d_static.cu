@@ -222,6 +222,7 @@ extern "C" int fft3d_filter2d_static(const fft3d_params* p0, const fft3d_plane_d
   fa.wan_x = tab.wan_x;
   fa.wan_y = tab.wan_y;
   fa.spec = spec;
+  for (int x = 0; x < fft3d::kMaxBw; x++) fa.wx[x] = x < ep.bw ? blob[o_wx + x] : 0.f;
   err = fft3d::launch_forward(fa, bytes, st);
   if (err != cudaSuccess) return sfail(FFT3D_E_CUDA, std::string("neo_fft3d: forward kernel: ") + cudaGetErrorString(err));
 
