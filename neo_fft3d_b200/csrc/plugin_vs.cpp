@@ -9,7 +9,11 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -17,6 +21,15 @@
 #include "fft3d_b200.h"
 
 namespace {
+
+// The outputs of one frame group (frames n0 .. n0 + k - 1), computed once by
+// whichever request gets there first and then served to the others.
+struct GroupOut {
+  std::mutex mu;
+  bool done = false;
+  std::string err;
+  std::vector<const VSFrameRef*> out;
+};
 
 struct FFT3DFilter {
   VSNodeRef* node = nullptr;
@@ -27,7 +40,17 @@ struct FFT3DFilter {
   bool crop = false;
   std::mutex pattern_lock;
   bool pattern_done = false;
+  // Frame groups (Wiener 3D, opt-in): a request for frame n filters its whole
+  // aligned group of `group` frames in one fft3d_plane_filter_frames call per
+  // plane and keeps the outputs for the group's other requests (`cache`, the
+  // most recent kCachedGroups groups). group <= 1: one frame per call.
+  int group = 1;
+  std::mutex cache_lock;
+  std::map<int, std::shared_ptr<GroupOut>> cache;
+  std::deque<int> cache_order;
 };
+
+constexpr int kCachedGroups = 6;
 
 // Reads an optional argument with the reference's VS semantics: absent keys
 // keep the default (include/dualsynth/vs_wrapper.hpp:114-137).
@@ -50,6 +73,9 @@ void VS_CC fft3d_init(VSMap*, VSMap*, void** instance, VSNode* node, VSCore*, co
 
 void VS_CC fft3d_free(void* instance, VSCore*, const VSAPI* api) {
   auto* d = static_cast<FFT3DFilter*>(instance);
+  for (auto& kv : d->cache)
+    for (auto* f : kv.second->out)
+      if (f) api->freeFrame(f);
   for (auto* h : d->plane)
     if (h) fft3d_plane_destroy(h);
   if (d->node) api->freeNode(d->node);
@@ -59,9 +85,150 @@ void VS_CC fft3d_free(void* instance, VSCore*, const VSAPI* api) {
 int plane_w(const VSVideoInfo& vi, int p) { return p ? vi.width >> vi.format->subSamplingW : vi.width; }
 int plane_h(const VSVideoInfo& vi, int p) { return p ? vi.height >> vi.format->subSamplingH : vi.height; }
 
+// Noise pattern from frame pframe, once, before the first filtered frame.
+std::string ensure_pattern(FFT3DFilter* d, VSFrameContext* ctx, const VSAPI* api) {
+  std::string err;
+  std::lock_guard<std::mutex> lk(d->pattern_lock);
+  if (d->pattern_done) return err;
+  const int last = d->vi.numFrames - 1;
+  const VSFrameRef* pf = api->getFrameFilter(std::min(std::max(d->p.pframe, 0), last), d->node, ctx);
+  for (int p = 0; p < d->vi.format->numPlanes && err.empty(); p++)
+    if (d->plane[p] && fft3d_plane_set_pattern_frame(d->plane[p], api->getReadPtr(pf, p), api->getStride(pf, p)))
+      err = fft3d_last_error();
+  api->freeFrame(pf);
+  d->pattern_done = true;
+  return err;
+}
+
+// The group's outputs: the window's frames (n0 - bt/2 .. n0 + k - 1 +
+// (bt-1)/2, as requested), one fft3d_plane_filter_frames call per processed
+// plane, the other planes copied.
+void compute_group(FFT3DFilter* d, GroupOut* e, int n0, int k, VSFrameContext* ctx, VSCore* core, const VSAPI* api) {
+  const VSFormat* fi = d->vi.format;
+  const int last = d->vi.numFrames - 1;
+  const int lo = std::max(n0 - d->p.bt / 2, 0), hi = std::min(n0 + k - 1 + (d->p.bt - 1) / 2, last);
+  std::vector<const VSFrameRef*> src(k + 4, nullptr);  // frame n0 - 2 + j
+  for (int m = lo; m <= hi; m++) src[m - (n0 - 2)] = api->getFrameFilter(m, d->node, ctx);
+  e->out.assign(k, nullptr);
+  for (int j = 0; j < k; j++) e->out[j] = api->newVideoFrame(fi, d->vi.width, d->vi.height, src[j + 2], core);
+  for (int p = 0; p < fi->numPlanes && e->err.empty(); p++) {
+    if (!d->plane[p]) {  // planes not processed are copied (process = 2)
+      const int rb = plane_w(d->vi, p) * fi->bytesPerSample;
+      for (int j = 0; j < k; j++) {
+        const uint8_t* sp = api->getReadPtr(src[j + 2], p);
+        uint8_t* dp = api->getWritePtr(const_cast<VSFrameRef*>(e->out[j]), p);
+        const int ss = api->getStride(src[j + 2], p), ds = api->getStride(e->out[j], p);
+        for (int y = 0; y < plane_h(d->vi, p); y++) std::memcpy(dp + (size_t)y * ds, sp + (size_t)y * ss, rb);
+      }
+      continue;
+    }
+    std::vector<const void*> ptrs(k + 4, nullptr);
+    std::vector<int> strides(k + 4, 0);
+    for (int j = 0; j < k + 4; j++)
+      if (src[j]) {
+        ptrs[j] = api->getReadPtr(src[j], p);
+        strides[j] = api->getStride(src[j], p);
+      }
+    std::vector<void*> dst(k);
+    std::vector<int> dstride(k);
+    for (int j = 0; j < k; j++) {
+      dst[j] = api->getWritePtr(const_cast<VSFrameRef*>(e->out[j]), p);
+      dstride[j] = api->getStride(e->out[j], p);
+    }
+    if (fft3d_plane_filter_frames(d->plane[p], n0, k, ptrs.data(), strides.data(), dst.data(), dstride.data()))
+      e->err = fft3d_last_error();
+  }
+  for (auto* f : src)
+    if (f) api->freeFrame(f);
+}
+
+const VSFrameRef* group_get_frame(FFT3DFilter* d, int n, int reason, VSFrameContext* ctx, VSCore* core,
+                                  const VSAPI* api) {
+  const int G = d->group, last = d->vi.numFrames - 1;
+  const int g = n / G, n0 = g * G, k = std::min(G, last + 1 - n0);
+  if (reason == arInitial) {
+    {
+      std::lock_guard<std::mutex> lk(d->cache_lock);
+      auto it = d->cache.find(g);
+      if (it != d->cache.end()) {
+        std::lock_guard<std::mutex> gl(it->second->mu);
+        if (it->second->done && it->second->err.empty()) return api->cloneFrameRef(it->second->out[n - n0]);
+      }
+    }
+    const int lo = std::max(n0 - d->p.bt / 2, 0), hi = std::min(n0 + k - 1 + (d->p.bt - 1) / 2, last);
+    for (int m = lo; m <= hi; m++) api->requestFrameFilter(m, d->node, ctx);
+    if (d->p.pfactor != 0 && !d->pattern_done)
+      api->requestFrameFilter(std::min(std::max(d->p.pframe, 0), last), d->node, ctx);
+    return nullptr;
+  }
+  if (reason != arAllFramesReady) return nullptr;
+  if (d->p.pfactor != 0) {
+    const std::string perr = ensure_pattern(d, ctx, api);
+    if (!perr.empty()) {
+      api->setFilterError(("FFT3D: " + perr).c_str(), ctx);
+      return nullptr;
+    }
+  }
+  std::shared_ptr<GroupOut> e;
+  {
+    std::lock_guard<std::mutex> lk(d->cache_lock);
+    auto& slot = d->cache[g];
+    if (!slot) {
+      slot = std::make_shared<GroupOut>();
+      d->cache_order.push_back(g);
+      while ((int)d->cache_order.size() > kCachedGroups) {
+        const int old = d->cache_order.front();
+        d->cache_order.pop_front();
+        auto it = d->cache.find(old);
+        if (it == d->cache.end()) continue;
+        // not while it is being computed; a request still holding it
+        // recomputes it (its window frames are requested)
+        std::lock_guard<std::mutex> gl(it->second->mu);
+        for (auto* f : it->second->out)
+          if (f) api->freeFrame(f);
+        it->second->out.clear();
+        it->second->done = false;
+        d->cache.erase(it);
+      }
+    }
+    e = slot;
+  }
+  std::string err;
+  const VSFrameRef* out = nullptr;
+  {
+    std::lock_guard<std::mutex> gl(e->mu);
+    if (!e->done) {
+      e->err.clear();
+      compute_group(d, e.get(), n0, k, ctx, core, api);
+      e->done = true;
+    }
+    if (e->err.empty()) {
+      out = api->cloneFrameRef(e->out[n - n0]);
+    } else {
+      err = e->err;
+      for (auto* f : e->out)
+        if (f) api->freeFrame(f);
+      e->out.clear();
+      e->done = false;
+    }
+  }
+  if (!err.empty()) {
+    {
+      // a failed group is not kept (lock order: cache, then group)
+      std::lock_guard<std::mutex> lk(d->cache_lock);
+      auto it = d->cache.find(g);
+      if (it != d->cache.end() && it->second == e) d->cache.erase(it);
+    }
+    api->setFilterError(("FFT3D: " + err).c_str(), ctx);
+    return nullptr;
+  }
+  return out;
+}
+
 const VSFrameRef* VS_CC fft3d_get_frame(int n, int reason, void** instance, void**, VSFrameContext* ctx, VSCore* core,
                                         const VSAPI* api) {
   auto* d = static_cast<FFT3DFilter*>(*instance);
+  if (d->group > 1) return group_get_frame(d, n, reason, ctx, core, api);
   const int bt = d->p.bt;
   const int last = d->vi.numFrames - 1;
   // frames of the temporal window, src/fft3d.hpp:201-219
@@ -200,6 +367,13 @@ void VS_CC fft3d_create(const VSMap* in, VSMap* out, void*, VSCore* core, const 
     pd.ssh = fi->subSamplingH;
     pd.num_frames = d->vi.numFrames;
     if (fft3d_plane_create(&p, &pd, 0, &d->plane[i])) return fail(fft3d_last_error());
+  }
+  // Wiener 3D: frame groups of NEO_FFT3D_FRAME_GROUP frames when set (off by
+  // default: with the core's pageable frame buffers the host copies bound the
+  // plugin, and a group serialises the copies of its frames' requests)
+  if (p.bt >= 2) {
+    const char* env = std::getenv("NEO_FFT3D_FRAME_GROUP");
+    d->group = env ? std::max(1, std::min(std::atoi(env), FFT3D_MAX_FRAME_GROUP)) : 1;
   }
   // Kalman is history-dependent: frames in order (src/fft3d.hpp:27-28)
   api->createFilter(in, out, "FFT3D", fft3d_init, fft3d_get_frame, fft3d_free, p.bt == 0 ? fmSerial : fmParallel, 0,

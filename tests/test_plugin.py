@@ -63,3 +63,27 @@ def test_plugin_parallel_render_matches_serial(gpu):
     b = c.invoke("neo_fft3d", "FFT3D", c.clip(planes), sigma=3.0, bt=5).render(threads=4)
     for x, y in zip(a, b):
         assert np.abs(x.astype(int) - y.astype(int)).max() <= 1
+
+
+@pytest.mark.gpu
+def test_plugin_frame_groups_match_one_frame_per_call(gpu, monkeypatch):
+    """With NEO_FFT3D_FRAME_GROUP set, the VapourSynth plugin filters Wiener
+    3D clips in frame groups (each request computes its aligned group once,
+    the group's other requests are served from the group): the same frames as
+    one frame per call, rendered by parallel workers and in reverse order."""
+    planes = synth.make_clip(176, 144, 21, noise_sigma=5, seed=47)
+    outs = []
+    for g, threads in (("1", 1), ("8", 4), ("3", 3), ("16", 1)):
+        monkeypatch.setenv("NEO_FFT3D_FRAME_GROUP", g)
+        c = ours()
+        outs.append(c.invoke("neo_fft3d", "FFT3D", c.clip(planes), sigma=3.0, bt=5, sharpen=0.2).render(threads=threads))
+    for o in outs[1:]:
+        for a, b in zip(outs[0], o):
+            assert np.array_equal(a, b)
+    monkeypatch.setenv("NEO_FFT3D_FRAME_GROUP", "8")
+    c = ours()
+    node = c.invoke("neo_fft3d", "FFT3D", c.clip(planes), sigma=3.0, bt=5, sharpen=0.2)
+    for n in reversed(range(21)):
+        got = node.render(first=n, count=1)
+        for a, b in zip(outs[0], got):
+            assert np.array_equal(a[n], b[0])
