@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -125,9 +126,20 @@ struct fft3d_plane {
     cudaEvent_t in_free = nullptr;   // the kernels reading `in` are done
     cudaEvent_t out_free = nullptr;  // the download of `out` is done
     int* h_flags = nullptr;          // pinned copies of the device error flags
+    // Pageable callers: the call's new frame, copied into pinned memory by
+    // the calling thread before the call is queued, and its result, read
+    // back through pinned memory and copied out after the call's wait
+    // (unpadded rows; allocated on first pageable use).
+    uint8_t* h_in = nullptr;
+    uint8_t* h_out = nullptr;
+    cudaEvent_t h_in_done = nullptr;   // the upload from h_in is done
+    const void* staged_src = nullptr;  // the caller's frame that h_in holds
+    bool pageable_out = false;         // this call downloads into h_out
+    bool busy = false;                 // owned by a call (stage_cv)
   };
-  static constexpr int kStages = 3;
+  static constexpr int kStages = 6;
   Stage stages[kStages];
+  std::condition_variable stage_cv;  // with pool_mu: a stage became free
   // Host frame groups (fft3d_plane_filter_frames): per call, the group's
   // uploaded frames and its outputs in pitched device planes (grown to the
   // largest group), used round robin like the one-frame stages.
@@ -318,6 +330,9 @@ void free_plane(fft3d_plane* P) {
   for (auto& sg : P->stages) {
     cudaFree(sg.in);
     cudaFree(sg.out);
+    if (sg.h_in) cudaFreeHost(sg.h_in);
+    if (sg.h_out) cudaFreeHost(sg.h_out);
+    if (sg.h_in_done) cudaEventDestroy(sg.h_in_done);
     if (sg.in_free) cudaEventDestroy(sg.in_free);
     if (sg.out_free) cudaEventDestroy(sg.out_free);
     if (sg.h_flags) cudaFreeHost(sg.h_flags);
@@ -428,11 +443,29 @@ int stream_after(fft3d_plane* P, cudaStream_t wait, cudaStream_t done_on) {
 // the kernels of stream `st` then wait for the copy.
 int upload_frame(fft3d_plane* P, const void* plane, int stride, cudaStream_t st) {
   fft3d_plane::Stage* sg = P->cur;
+  const size_t row = (size_t)P->d.width * P->bytes;
   CK(cudaStreamWaitEvent(P->s_up, sg->in_free, 0), "event");
-  CK(cudaMemcpy2DAsync(sg->in, sg->in_pitch, plane, stride, (size_t)P->d.width * P->bytes, P->d.height,
-                       cudaMemcpyHostToDevice, P->s_up),
-     "frame upload");
+  if (sg->staged_src && plane == sg->staged_src) {
+    // the frame the caller's thread already copied into pinned memory
+    CK(cudaMemcpy2DAsync(sg->in, sg->in_pitch, sg->h_in, row, row, P->d.height, cudaMemcpyHostToDevice, P->s_up),
+       "frame upload");
+    CK(cudaEventRecord(sg->h_in_done, P->s_up), "event");
+    sg->staged_src = nullptr;
+  } else {
+    CK(cudaMemcpy2DAsync(sg->in, sg->in_pitch, plane, stride, row, P->d.height, cudaMemcpyHostToDevice, P->s_up),
+       "frame upload");
+  }
   return stream_after(P, st, P->s_up);
+}
+
+// Whether host memory p is pinned (page-locked or registered).
+bool host_pinned(const void* p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
 }
 
 // The spectrum of frame m in a ring slot, computing it from `plane` if needed.
@@ -665,8 +698,13 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
     if (rc) return rc;
     char* hdst = static_cast<char*>(dst) + (size_t)P->t * dst_stride + (size_t)P->l * P->bytes;
     const char* ddst = static_cast<const char*>(sg->out) + P->t * sg->out_pitch + (size_t)P->l * P->bytes;
-    CK(cudaMemcpy2DAsync(hdst, dst_stride, ddst, sg->out_pitch, (size_t)P->g.W * P->bytes, P->g.H,
-                         cudaMemcpyDeviceToHost, P->s_down), "result download");
+    const size_t orow = (size_t)P->g.W * P->bytes;
+    if (sg->pageable_out)  // into pinned memory; the caller's thread copies it out after its wait
+      CK(cudaMemcpy2DAsync(sg->h_out, orow, ddst, sg->out_pitch, orow, P->g.H, cudaMemcpyDeviceToHost, P->s_down),
+         "result download");
+    else
+      CK(cudaMemcpy2DAsync(hdst, dst_stride, ddst, sg->out_pitch, orow, P->g.H, cudaMemcpyDeviceToHost, P->s_down),
+         "result download");
     CK(cudaEventRecord(sg->out_free, P->s_down), "event");
     sg->h_flags[0] = sg->h_flags[1] = 0;
     CK(cudaMemcpyAsync(&sg->h_flags[0], P->d_err, sizeof(int), cudaMemcpyDeviceToHost, P->s_down), "error flag");
@@ -676,6 +714,72 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
     P->call_done = take_sync_event(P);
     CK(cudaEventRecord(P->call_done, P->s_down), "event");
   }
+  return FFT3D_OK;
+}
+
+// A stage for one host-path call, exclusive until the call returns (the
+// stages are used round robin; a call waits while all are owned).
+fft3d_plane::Stage* acquire_stage(fft3d_plane* P) {
+  std::unique_lock<std::mutex> lk(P->pool_mu);
+  for (;;) {
+    for (int k = 0; k < fft3d_plane::kStages; k++) {
+      const int i = (P->next_stage + k) % fft3d_plane::kStages;
+      if (!P->stages[i].busy) {
+        P->stages[i].busy = true;
+        P->next_stage = (i + 1) % fft3d_plane::kStages;
+        return &P->stages[i];
+      }
+    }
+    P->stage_cv.wait(lk);
+  }
+}
+
+void release_stage(fft3d_plane* P, fft3d_plane::Stage* sg) {
+  {
+    std::lock_guard<std::mutex> lk(P->pool_mu);
+    sg->busy = false;
+  }
+  P->stage_cv.notify_one();
+}
+
+// Pageable host buffers of a one-frame call: the window's newest frame, if
+// the plane will need it and it is pageable, is copied into the stage's
+// pinned input by the calling thread (outside the plane's lock), and a
+// pageable destination gets its result through the stage's pinned output.
+int stage_pageable(fft3d_plane* P, fft3d_plane::Stage* sg, int n, const void* const src[5], const int stride[5],
+                   void* dst) {
+  sg->staged_src = nullptr;
+  sg->pageable_out = !host_pinned(dst);
+  const size_t row = (size_t)P->d.width * P->bytes, plane = row * P->d.height;
+  const size_t orow = (size_t)P->g.W * P->bytes, oplane = orow * P->g.H;
+  if (sg->pageable_out && !sg->h_out && cudaMallocHost(&sg->h_out, oplane) != cudaSuccess) {
+    cudaGetLastError();
+    sg->h_out = nullptr;
+    sg->pageable_out = false;  // the driver copies instead
+  }
+  if (!src) return FFT3D_OK;
+  const int bt = P->ep.bt;
+  int to = 0;
+  if (bt > 1 && !((bt / 2 > n) || (bt - 1) / 2 > (P->d.num_frames - 1 - n))) to = (bt - 1) / 2;
+  const void* fsrc = src[2 + to];
+  if (!fsrc || (bt == 0 && n == 0)) return FFT3D_OK;
+  {
+    std::lock_guard<std::mutex> lk(P->mu);
+    if (find_slot(P, n + to)) return FFT3D_OK;  // cached: nothing to upload
+  }
+  if (host_pinned(fsrc)) return FFT3D_OK;
+  if (!sg->h_in) {
+    if (cudaMallocHost(&sg->h_in, plane) != cudaSuccess ||
+        cudaEventCreateWithFlags(&sg->h_in_done, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      return FFT3D_OK;  // the driver copies instead
+    }
+  } else {
+    CK(cudaEventSynchronize(sg->h_in_done), "staging");  // its last upload is done
+  }
+  for (int y = 0; y < P->d.height; y++)
+    std::memcpy(sg->h_in + (size_t)y * row, static_cast<const char*>(fsrc) + (size_t)y * stride[2 + to], row);
+  sg->staged_src = fsrc;
   return FFT3D_OK;
 }
 
@@ -1332,19 +1436,29 @@ int fft3d_plane_filter(fft3d_plane* P, int n, const void* const src[5], const in
                        int dst_stride) {
   if (!P || !dst) return fail(FFT3D_E_PARAM, "neo_fft3d: null argument");
   cudaEvent_t done = nullptr;
-  fft3d_plane::Stage* sg = nullptr;
   bool learned = false;
+  // the call owns a stage until its result is in dst
+  fft3d_plane::Stage* sg = acquire_stage(P);
+  struct Release {
+    fft3d_plane* P;
+    fft3d_plane::Stage* sg;
+    ~Release() { release_stage(P, sg); }
+  } release{P, sg};
+  CK(cudaSetDevice(P->device), "cudaSetDevice");
+  // Pageable frames (e.g. a frame server's buffers) would be copied by the
+  // driver while the plane is locked: the new frame is copied here into
+  // pinned memory first, and the result comes back through pinned memory.
+  int rc = stage_pageable(P, sg, n, src, src_stride, dst);
+  if (rc) return rc;
   {
     std::lock_guard<std::mutex> lk(P->mu);
-    CK(cudaSetDevice(P->device), "cudaSetDevice");
-    sg = &P->stages[P->next_stage];
-    P->next_stage = (P->next_stage + 1) % fft3d_plane::kStages;
     P->cur = sg;
     P->call_done = nullptr;
-    const int rc = run_filter(P, n, src, src_stride, dst, dst_stride, true, P->stream);
+    rc = run_filter(P, n, src, src_stride, dst, dst_stride, true, P->stream);
     done = P->call_done;
     P->call_done = nullptr;
     P->cur = nullptr;
+    sg->staged_src = nullptr;
     learned = P->psd_model != nullptr;
     if (rc) {
       if (done) {
@@ -1356,7 +1470,13 @@ int fft3d_plane_filter(fft3d_plane* P, int n, const void* const src[5], const in
   }
   if (!done) return FFT3D_OK;  // answered on the host (Kalman frame 0)
   cudaSetDevice(P->device);
-  return finish_call(P, done, sg, learned);
+  rc = finish_call(P, done, sg, learned);
+  if (rc == FFT3D_OK && sg->pageable_out) {
+    const size_t orow = (size_t)P->g.W * P->bytes;
+    char* hdst = static_cast<char*>(dst) + (size_t)P->t * dst_stride + (size_t)P->l * P->bytes;
+    for (int y = 0; y < P->g.H; y++) std::memcpy(hdst + (size_t)y * dst_stride, sg->h_out + (size_t)y * orow, orow);
+  }
+  return rc;
 }
 
 int fft3d_plane_filter_device(fft3d_plane* P, int n, const void* const src[5], const int src_stride[5], void* dst,
