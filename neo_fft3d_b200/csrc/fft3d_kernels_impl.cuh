@@ -394,9 +394,13 @@ __device__ __forceinline__ float2 filter_vals(const InverseArgs& a, const float2
   if constexpr (MODE == MODE_SHARPEN_ONLY) {
     return cur;
   } else if constexpr (MODE == MODE_KALMAN) {
-    // src/code_impl/Kalman.cpp:27-64
-    float2 last = a.kal_last[off + bin];
-    float cv = a.kal_covar[off + bin], cp = a.kal_covarp[off + bin];
+    // src/code_impl/Kalman.cpp:27-64; the state is read once and written
+    // back by this thread: coherent loads that do not allocate in L1
+    float2 last;
+    float cv, cp;
+    asm("ld.global.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(last.x), "=f"(last.y) : "l"(a.kal_last + off + bin));
+    asm("ld.global.L1::no_allocate.f32 %0, [%1];" : "=f"(cv) : "l"(a.kal_covar + off + bin));
+    asm("ld.global.L1::no_allocate.f32 %0, [%1];" : "=f"(cp) : "l"(a.kal_covarp + off + bin));
     float sigma = a.c.sigma2n_2d;
     if (a.psd) {
       sigma = learned_noise(a, off, bin);
