@@ -59,6 +59,7 @@ typedef struct fft3d_plane_desc {
   int is_chroma;       /* YUV chroma plane: integer samples are centred on 2^(bits-1) */
   int ssw, ssh;        /* subsampling shifts applied to the crop l/r and t/b */
   int num_frames;      /* clip length; frames near either end use bt = 1 */
+  int rgb;             /* plane of an RGB clip (pshow's display offset; 0 for YUV and Gray) */
 } fft3d_plane_desc;
 
 typedef struct fft3d_plane fft3d_plane;
@@ -137,7 +138,8 @@ int fft3d_plane_geometry(fft3d_plane* h, int out[8]);
  * the reference does from frame pframe on its first GetFrame
  * (src/fft3d_engine.h:485-504, src/helper.cpp:46-132): block (px, py), or the
  * quietest block when px = py = 0. Required before the first filter call of a
- * pattern-mode plane; a no-op otherwise. */
+ * pattern-mode plane; a no-op otherwise, and for pshow planes, which find the
+ * block on every frame. */
 int fft3d_plane_set_pattern_frame(fft3d_plane* h, const void* src, int src_stride);
 
 /* Drop all cached spectra and reset the Kalman state to its initial values.

@@ -101,6 +101,11 @@ struct fft3d_plane {
   // (device-buffer calls, batch steps): fft3d_plane_reset waits for it
   // before it clears the ring and the Kalman state
   cudaEvent_t last_work = nullptr;
+  // pshow: spectrum scratch, constant-1 windows, and whether the windows have
+  // become constant (after the first pshow frame)
+  float2* d_pshow = nullptr;
+  float* d_pshow_win = nullptr;
+  bool pshow_flat = false;
   // a reset queued on `stream` that the next call must wait for (on its own
   // stream) before it reads the ring or the Kalman state
   cudaEvent_t reset_done = nullptr;
@@ -316,6 +321,8 @@ void free_plane(fft3d_plane* P) {
   for (auto& s : P->slots) cudaFree(s.spec);
   cudaFree(P->d_tables);
   cudaFree(P->d_tdom);
+  cudaFree(P->d_pshow);
+  cudaFree(P->d_pshow_win);
   for (auto* t : P->tdom_extra) cudaFree(t);
   cudaFree(P->d_filt);
   cudaFree(P->d_tc);
@@ -507,6 +514,190 @@ int copy_plane(fft3d_plane* P, void* dst, int dstride, const void* src, int sstr
   return FFT3D_OK;
 }
 
+// The output of one frame from its time-domain blocks: the crop borders from
+// the source frame (src/fft3d.hpp:292-352), the overlap-add with the tables'
+// synthesis windows and sample offset `base`, and on the host path the
+// download of the result on its own stream.
+int output_frame(fft3d_plane* P, float* tdom, const fft3d::Tables& tab, float base, void* dst, int dst_stride,
+                 const void* cur, int cur_stride, bool host, bool learned, cudaStream_t st) {
+  const fft3d_params& ep = P->ep;
+  const bool crop = ep.l > 0 || ep.t > 0 || ep.r > 0 || ep.b > 0;
+  void* odst = dst;
+  long long ostride = dst_stride;
+  if (host) {
+    odst = P->cur->out;
+    ostride = (long long)P->cur->out_pitch;
+    // the stage's previous result must have been downloaded
+    CK(cudaStreamWaitEvent(st, P->cur->out_free, 0), "event");
+    if (crop) {
+      if (!cur) return fail(FFT3D_E_FRAME, "neo_fft3d: the current frame is needed for the crop borders");
+      for (int y = 0; y < P->d.height; y++)
+        std::memcpy(static_cast<char*>(dst) + (size_t)y * dst_stride, static_cast<const char*>(cur) + (size_t)y * cur_stride,
+                    (size_t)P->d.width * P->bytes);
+    }
+  } else if (crop) {
+    if (!cur) return fail(FFT3D_E_FRAME, "neo_fft3d: the current frame is needed for the crop borders");
+    int rc = copy_plane(P, dst, dst_stride, cur, cur_stride, cudaMemcpyDeviceToDevice, st);
+    if (rc) return rc;
+  }
+  fft3d::OlaArgs oa;
+  oa.g = P->g;
+  oa.t = tab;
+  oa.tdom = tdom;
+  oa.dst = static_cast<char*>(odst) + (long long)P->t * ostride + (long long)P->l * P->bytes;
+  oa.dst_stride = ostride;
+  oa.norm = P->norm;
+  const bool ints = P->bytes != 4;
+  oa.rounder = ints ? 0.5f : 0.f;
+  oa.base = base;
+  oa.maxval = P->bytes == 1 ? 255 : (1 << P->d.bits) - 1;
+  if (g_defer) {
+    g_defer->ola.push_back({oa, P->bytes, g_defer->plane});
+  } else {
+    TimeScope ts(P, K_OLA, (double)P->g.nblocks * P->g.bh * P->g.bw * 4 + (double)P->g.W * P->g.H * P->bytes, st);
+    CK(fft3d::launch_overlap_add(oa, P->bytes, st), "overlap-add kernel");
+    g_launches++;
+  }
+  if (host) {
+    // download on its own stream once the kernels are done; then the error
+    // flags; the caller waits on the call's completion event
+    fft3d_plane::Stage* sg = P->cur;
+    int rc = stream_after(P, P->s_down, st);
+    if (rc) return rc;
+    char* hdst = static_cast<char*>(dst) + (size_t)P->t * dst_stride + (size_t)P->l * P->bytes;
+    const char* ddst = static_cast<const char*>(sg->out) + P->t * sg->out_pitch + (size_t)P->l * P->bytes;
+    const size_t orow = (size_t)P->g.W * P->bytes;
+    if (sg->pageable_out)  // into pinned memory; the caller's thread copies it out after its wait
+      CK(cudaMemcpy2DAsync(sg->h_out, orow, ddst, sg->out_pitch, orow, P->g.H, cudaMemcpyDeviceToHost, P->s_down),
+         "result download");
+    else
+      CK(cudaMemcpy2DAsync(hdst, dst_stride, ddst, sg->out_pitch, orow, P->g.H, cudaMemcpyDeviceToHost, P->s_down),
+         "result download");
+    CK(cudaEventRecord(sg->out_free, P->s_down), "event");
+    sg->h_flags[0] = sg->h_flags[1] = 0;
+    CK(cudaMemcpyAsync(&sg->h_flags[0], P->d_err, sizeof(int), cudaMemcpyDeviceToHost, P->s_down), "error flag");
+    if (learned)
+      CK(cudaMemcpyAsync(&sg->h_flags[1], fft3d::psd::err_flag(P->psd_model), sizeof(int), cudaMemcpyDeviceToHost,
+                         P->s_down), "error flag");
+    P->call_done = take_sync_event(P);
+    CK(cudaEventRecord(P->call_done, P->s_down), "event");
+  }
+  return FFT3D_OK;
+}
+
+// FindPatternBlock (src/helper.cpp:46-90) on the spectra `spec`: the interior
+// block with the least windowed power, scored on the device in the
+// reference's summation order; the first minimum in raster order wins, as in
+// the reference's loop. *px, *py are left unchanged when the plane has no
+// interior block. Synchronises stream st.
+int find_pattern_block(fft3d_plane* P, const float2* spec, cudaStream_t st, int* px, int* py) {
+  const int nb = P->g.bh * P->g.nh;
+  const int wx = P->g.nox - 4, wy = P->g.noy - 4;
+  if (wx <= 0 || wy <= 0) return FFT3D_OK;
+  float* d_buf = nullptr;
+  CK(cudaMalloc(&d_buf, ((size_t)wx * wy + nb) * sizeof(float)), "pattern scores");
+  std::vector<float> scores((size_t)wx * wy);
+  cudaError_t e = cudaMemcpyAsync(d_buf + (size_t)wx * wy, P->h_pwin.data(), nb * sizeof(float),
+                                  cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = fft3d::launch_pattern_scores(spec, P->tab.grid, d_buf + (size_t)wx * wy, P->g.nox, P->g.noy, nb, P->ep.degrid,
+                                     d_buf, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(scores.data(), d_buf, scores.size() * sizeof(float), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(d_buf);
+  if (e != cudaSuccess) return cuda_fail(e, "pattern scores");
+  float best = 1e15f;
+  for (size_t k = 0; k < scores.size(); k++)
+    if (scores[k] < best) {
+      best = scores[k];
+      *px = 2 + (int)(k % wx);
+      *py = 2 + (int)(k / wx);
+    }
+  return FFT3D_OK;
+}
+
+// pshow (src/fft3d_engine.h:505-565): instead of the filtered frame, the noise
+// pattern's block alone. The block is found on frame n itself (or is px, py);
+// from then on the analysis and synthesis windows are constant 1, as the
+// reference overwrites them; frame n is transformed again with those windows
+// and a sample offset of 2^(bits-1) for every plane of a non-RGB clip (the
+// reference's CoverToOverlap flag there is "not RGB"), every other block's
+// spectrum is zeroed (PutPatternOnly, src/helper.cpp:134-170), and the
+// inverse and overlap-add give the block's pixels on a flat background. The
+// reference's caption is a TODO there and is not drawn.
+int pshow_frame(fft3d_plane* P, int n, const void* const src[5], const int stride[5], void* dst, int dst_stride,
+                bool host, cudaStream_t st) {
+  (void)n;
+  const void* cur = src ? src[2] : nullptr;
+  if (!cur) return fail(FFT3D_E_FRAME, "neo_fft3d: frame " + std::to_string(n) + " is needed but was not supplied");
+  const size_t spec_bytes = P->spec_elems() * sizeof(float2);
+  if (!P->d_pshow) {
+    const int nt = P->g.bw + P->g.bh + 2 * P->g.ow + 2 * P->g.oh;
+    float* t = nullptr;
+    if (cudaMalloc(&P->d_pshow, spec_bytes) != cudaSuccess || cudaMalloc(&t, nt * sizeof(float)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (pshow)");
+    }
+    P->d_pshow_win = t;
+    std::vector<float> ones(nt, 1.f);
+    CK(cudaMemcpy(t, ones.data(), nt * sizeof(float), cudaMemcpyHostToDevice), "pshow tables");
+  }
+  const void* plane = cur;
+  long long pstride = stride[2];
+  if (host) {
+    int rc = upload_frame(P, cur, stride[2], st);
+    if (rc) return rc;
+    plane = P->cur->in;
+    pstride = (long long)P->cur->in_pitch;
+  }
+  const float* ones = P->d_pshow_win;
+  auto forward = [&](bool constant, float base) {
+    fft3d::ForwardArgs a = forward_args(P, plane, pstride, P->d_pshow);
+    if (constant) {
+      a.wan_x = ones;
+      a.wan_y = ones;
+      for (float& w : a.wx) w = 1.f;
+    }
+    a.base = base;
+    g_launches++;
+    return fft3d::launch_forward(a, P->bytes, st);
+  };
+  const bool ints = P->bytes != 4;
+  const float half = ints ? (float)(1 << (P->d.bits - 1)) : 0.f;
+  // the block: on frame n with the current windows and the plane's own offset
+  int pxf = P->ep.px, pyf = P->ep.py;
+  CK(forward(P->pshow_flat, P->d.is_chroma ? half : 0.f), "forward kernel (pshow)");
+  if (P->ep.px == 0 && P->ep.py == 0) {
+    int rc = find_pattern_block(P, P->d_pshow, st, &pxf, &pyf);
+    if (rc) return rc;
+  }
+  P->pshow_flat = true;
+  // the frame with constant windows; every block but the pattern's zeroed
+  const float base = P->d.rgb ? 0.f : half;
+  CK(forward(true, base), "forward kernel (pshow)");
+  const size_t nb = (size_t)P->g.bh * P->g.nh, blk = (size_t)pyf * P->g.nox + pxf;
+  if (blk > 0) CK(cudaMemsetAsync(P->d_pshow, 0, blk * nb * sizeof(float2), st), "pshow");
+  if (blk + 1 < (size_t)P->g.nblocks)
+    CK(cudaMemsetAsync(P->d_pshow + (blk + 1) * nb, 0, ((size_t)P->g.nblocks - blk - 1) * nb * sizeof(float2), st),
+       "pshow");
+  if (host) CK(cudaEventRecord(P->cur->in_free, st), "event");
+  fft3d::Tables tab = P->tab;
+  tab.wan_x = ones;
+  tab.wan_y = ones;
+  tab.wsyn_xl = tab.wsyn_xr = ones;
+  tab.wsyn_yl = tab.wsyn_yr = ones;
+  fft3d::InverseArgs ia{};
+  ia.g = P->g;
+  ia.t = tab;
+  ia.in[2] = P->d_pshow;
+  ia.tdom = P->d_tdom;
+  ia.err = P->d_err;
+  CK(fft3d::launch_filter_inverse(ia, fft3d::MODE_SHARPEN_ONLY, st), "inverse kernel (pshow)");
+  g_launches++;
+  return output_frame(P, P->d_tdom, tab, base, dst, dst_stride, cur, stride[2], host, false, st);
+}
+
 int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride[5], void* dst, int dst_stride,
                bool host, cudaStream_t st) {
   if (P->reset_pending) {  // fft3d_plane_reset queued on the plane's stream
@@ -514,6 +705,8 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
     P->reset_pending = false;
   }
   const fft3d_params& ep = P->ep;
+  // pshow shows the pattern block before any filtering (src/fft3d_engine.h:505)
+  if (ep.pshow && ep.pfactor != 0) return pshow_frame(P, n, src, stride, dst, dst_stride, host, st);
   const int bt = ep.bt;
   int btcur = bt;  // src/fft3d_engine.h:579-582
   if ((bt / 2 > n) || (bt - 1) / 2 > (P->d.num_frames - 1 - n)) btcur = 1;
@@ -652,69 +845,9 @@ int run_filter(fft3d_plane* P, int n, const void* const src[5], const int stride
     news->stamp = ++P->clock;
   }
   if (!g_defer) g_launches++;
-  // output: the crop borders come from the source frame (src/fft3d.hpp:292-352)
-  const bool crop = ep.l > 0 || ep.t > 0 || ep.r > 0 || ep.b > 0;
-  void* odst = dst;
-  long long ostride = dst_stride;
-  if (host) {
-    odst = P->cur->out;
-    ostride = (long long)P->cur->out_pitch;
-    // the stage's previous result must have been downloaded
-    CK(cudaStreamWaitEvent(st, P->cur->out_free, 0), "event");
-    if (crop) {
-      if (!cur) return fail(FFT3D_E_FRAME, "neo_fft3d: the current frame is needed for the crop borders");
-      for (int y = 0; y < P->d.height; y++)
-        std::memcpy(static_cast<char*>(dst) + (size_t)y * dst_stride, static_cast<const char*>(cur) + (size_t)y * stride[2],
-                    (size_t)P->d.width * P->bytes);
-    }
-  } else if (crop) {
-    if (!cur) return fail(FFT3D_E_FRAME, "neo_fft3d: the current frame is needed for the crop borders");
-    int rc = copy_plane(P, dst, dst_stride, cur, stride[2], cudaMemcpyDeviceToDevice, st);
-    if (rc) return rc;
-  }
-  fft3d::OlaArgs oa;
-  oa.g = P->g;
-  oa.t = P->tab;
-  oa.tdom = tdom;
-  oa.dst = static_cast<char*>(odst) + (long long)P->t * ostride + (long long)P->l * P->bytes;
-  oa.dst_stride = ostride;
-  oa.norm = P->norm;
   const bool ints = P->bytes != 4;
-  oa.rounder = ints ? 0.5f : 0.f;
-  oa.base = (ints && P->d.is_chroma) ? (float)(1 << (P->d.bits - 1)) : 0.f;
-  oa.maxval = P->bytes == 1 ? 255 : (1 << P->d.bits) - 1;
-  if (g_defer) {
-    g_defer->ola.push_back({oa, P->bytes, g_defer->plane});
-  } else {
-    TimeScope ts(P, K_OLA, (double)P->g.nblocks * P->g.bh * P->g.bw * 4 + (double)P->g.W * P->g.H * P->bytes, st);
-    CK(fft3d::launch_overlap_add(oa, P->bytes, st), "overlap-add kernel");
-    g_launches++;
-  }
-  if (host) {
-    // download on its own stream once the kernels are done; then the error
-    // flags; the caller waits on the call's completion event
-    fft3d_plane::Stage* sg = P->cur;
-    int rc = stream_after(P, P->s_down, st);
-    if (rc) return rc;
-    char* hdst = static_cast<char*>(dst) + (size_t)P->t * dst_stride + (size_t)P->l * P->bytes;
-    const char* ddst = static_cast<const char*>(sg->out) + P->t * sg->out_pitch + (size_t)P->l * P->bytes;
-    const size_t orow = (size_t)P->g.W * P->bytes;
-    if (sg->pageable_out)  // into pinned memory; the caller's thread copies it out after its wait
-      CK(cudaMemcpy2DAsync(sg->h_out, orow, ddst, sg->out_pitch, orow, P->g.H, cudaMemcpyDeviceToHost, P->s_down),
-         "result download");
-    else
-      CK(cudaMemcpy2DAsync(hdst, dst_stride, ddst, sg->out_pitch, orow, P->g.H, cudaMemcpyDeviceToHost, P->s_down),
-         "result download");
-    CK(cudaEventRecord(sg->out_free, P->s_down), "event");
-    sg->h_flags[0] = sg->h_flags[1] = 0;
-    CK(cudaMemcpyAsync(&sg->h_flags[0], P->d_err, sizeof(int), cudaMemcpyDeviceToHost, P->s_down), "error flag");
-    if (learned)
-      CK(cudaMemcpyAsync(&sg->h_flags[1], fft3d::psd::err_flag(P->psd_model), sizeof(int), cudaMemcpyDeviceToHost,
-                         P->s_down), "error flag");
-    P->call_done = take_sync_event(P);
-    CK(cudaEventRecord(P->call_done, P->s_down), "event");
-  }
-  return FFT3D_OK;
+  return output_frame(P, tdom, P->tab, (ints && P->d.is_chroma) ? (float)(1 << (P->d.bits - 1)) : 0.f, dst,
+                      dst_stride, cur, stride ? stride[2] : 0, host, learned, st);
 }
 
 // A stage for one host-path call, exclusive until the call returns (the
@@ -962,6 +1095,7 @@ std::string plane_batchable(const fft3d_plane* P) {
   if (P->d_tc) return "tensor-core planes are not batched";
   if (P->psd_model) return "planes with a learned noise PSD are not batched";
   if (P->bulk) return "the bulk-staged inverse is not batched";
+  if (P->ep.pshow && P->ep.pfactor != 0) return "pshow planes are not batched";
   return "";
 }
 
@@ -997,7 +1131,8 @@ int check_group_args(const fft3d_plane* P, int count, const void* const* src, co
 // Wiener 3D frames and one launch per frame otherwise (Kalman, whose state
 // runs from frame to frame, in frame order).
 bool group_path(const fft3d_plane* P, int count) {
-  return count > 1 && (P->path == 1 || P->path == 3) && !P->psd_model && !P->bulk;
+  return count > 1 && (P->path == 1 || P->path == 3) && !P->psd_model && !P->bulk &&
+         !(P->ep.pshow && P->ep.pfactor != 0);
 }
 
 // Frames n0 .. n0 + count - 1 from device frames (the window of frame n0 + j
@@ -1240,7 +1375,7 @@ int fft3d_plane_create(const fft3d_params* p, const fft3d_plane_desc* d, int dev
     return fail(FFT3D_E_UNSUPPORTED, "neo_fft3d: block size " + std::to_string(ep.bw) + "x" + std::to_string(ep.bh) +
                                          " is not built into this library (bw, bh in 8,12,16,24,32,48)");
   }
-  if (ep.pshow) { delete P; return fail(FFT3D_E_UNSUPPORTED, "neo_fft3d: pshow is not supported by the GPU engine"); }
+
   // crop in plane units, src/buffer.cpp:564-570
   P->l = d->is_chroma ? (ep.l >> d->ssw) : ep.l;
   int r = d->is_chroma ? (ep.r >> d->ssw) : ep.r;
@@ -1550,7 +1685,8 @@ int fft3d_plane_geometry(fft3d_plane* P, int out[8]) {
 int fft3d_plane_set_pattern_frame(fft3d_plane* P, const void* src, int stride) {
   if (!P || !src) return fail(FFT3D_E_PARAM, "neo_fft3d: null argument");
   std::lock_guard<std::mutex> lk(P->mu);
-  if (!P->pattern) return FFT3D_OK;
+  // pshow finds the pattern block on every frame itself (src/fft3d_engine.h:505-527)
+  if (!P->pattern || P->ep.pshow) return FFT3D_OK;
   CK(cudaSetDevice(P->device), "cudaSetDevice");
   // host-path calls still in flight may be using the first stage
   for (auto* st : {P->s_up, P->stream, P->s_down}) CK(cudaStreamSynchronize(st), "synchronize");
@@ -1562,32 +1698,8 @@ int fft3d_plane_set_pattern_frame(fft3d_plane* P, const void* src, int stride) {
   if (rc) return rc;
   const int nb = P->g.bh * P->g.nh;
   if (P->ep.px == 0 && P->ep.py == 0) {
-    // FindPatternBlock (src/helper.cpp:46-90): the interior block with the least
-    // windowed power, scored on the device in the reference's summation order;
-    // the first minimum in raster order wins, as in the reference's loop
-    const int wx = P->g.nox - 4, wy = P->g.noy - 4;
-    if (wx > 0 && wy > 0) {
-      float* d_buf = nullptr;
-      CK(cudaMalloc(&d_buf, ((size_t)wx * wy + nb) * sizeof(float)), "pattern scores");
-      std::vector<float> scores((size_t)wx * wy);
-      cudaError_t e = cudaMemcpyAsync(d_buf + (size_t)wx * wy, P->h_pwin.data(), nb * sizeof(float),
-                                      cudaMemcpyHostToDevice, P->stream);
-      if (e == cudaSuccess)
-        e = fft3d::launch_pattern_scores(s->spec, P->tab.grid, d_buf + (size_t)wx * wy, P->g.nox, P->g.noy, nb,
-                                         P->ep.degrid, d_buf, P->stream);
-      if (e == cudaSuccess)
-        e = cudaMemcpyAsync(scores.data(), d_buf, scores.size() * sizeof(float), cudaMemcpyDeviceToHost, P->stream);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(P->stream);
-      cudaFree(d_buf);
-      if (e != cudaSuccess) return cuda_fail(e, "pattern scores");
-      float best = 1e15f;
-      for (size_t k = 0; k < scores.size(); k++)
-        if (scores[k] < best) {
-          best = scores[k];
-          P->ep.px = 2 + (int)(k % wx);
-          P->ep.py = 2 + (int)(k / wx);
-        }
-    }
+    rc = find_pattern_block(P, s->spec, P->stream, &P->ep.px, &P->ep.py);
+    if (rc) return rc;
   }
   std::vector<float2> blk(nb);
   CK(cudaMemcpyAsync(blk.data(), s->spec + ((size_t)P->ep.py * P->g.nox + P->ep.px) * nb, nb * sizeof(float2),

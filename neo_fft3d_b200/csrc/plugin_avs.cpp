@@ -54,6 +54,7 @@ class NeoFFT3D : public GenericVideoFilter {
       d.ssw = ssw;
       d.ssh = ssh;
       d.num_frames = vi.num_frames;
+      d.rgb = yuv_ ? 0 : 1;
       if (fft3d_plane_create(&p_, &d, 0, &plane_[i])) {
         Fail f{fft3d_last_error()};
         release();

@@ -366,6 +366,7 @@ void VS_CC fft3d_create(const VSMap* in, VSMap* out, void*, VSCore* core, const 
     pd.ssw = fi->subSamplingW;
     pd.ssh = fi->subSamplingH;
     pd.num_frames = d->vi.numFrames;
+    pd.rgb = fi->colorFamily == cmRGB ? 1 : 0;
     if (fft3d_plane_create(&p, &pd, 0, &d->plane[i])) return fail(fft3d_last_error());
   }
   // Wiener 3D: frame groups of NEO_FFT3D_FRAME_GROUP frames when set (off by

@@ -33,7 +33,7 @@ class FFT3DParams(ctypes.Structure):
 class PlaneDesc(ctypes.Structure):
     _fields_ = [("width", ctypes.c_int), ("height", ctypes.c_int), ("bits", ctypes.c_int),
                 ("is_chroma", ctypes.c_int), ("ssw", ctypes.c_int), ("ssh", ctypes.c_int),
-                ("num_frames", ctypes.c_int)]
+                ("num_frames", ctypes.c_int), ("rgb", ctypes.c_int)]
 
 
 DEFAULTS = dict(sigma=2.0, beta=1.0, bw=32, bh=32, bt=3, ow=-1, oh=-1, kratio=2.0, sharpen=0.0, scutoff=0.3,
@@ -70,7 +70,7 @@ def plane_descs(planes_shapes, bits: int, num_frames: int, yuv: bool = True):
     for i, (h, w) in enumerate(planes_shapes):
         ssw = 0 if i == 0 else max(0, (w0 // w).bit_length() - 1)
         ssh = 0 if i == 0 else max(0, (h0 // h).bit_length() - 1)
-        out.append(PlaneDesc(w, h, bits, 1 if (yuv and 0 < i < 3) else 0, ssw, ssh, num_frames))
+        out.append(PlaneDesc(w, h, bits, 1 if (yuv and 0 < i < 3) else 0, ssw, ssh, num_frames, 0 if yuv else 1))
     return out
 
 
