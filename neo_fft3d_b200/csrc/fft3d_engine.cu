@@ -113,16 +113,13 @@ struct fft3d_plane {
   float2* d_last = nullptr;
   float* d_cov = nullptr;
   float* d_covp = nullptr;
-  void* d_in = nullptr;   // staging of host frames (whole plane): the first stage's
-  size_t in_pitch = 0;
-  void* d_out = nullptr;  // staging of the host output (whole plane): the first stage's
-  size_t out_pitch = 0;
-  // Host path (fft3d_plane_filter): staging planes used round robin by the
-  // calls, uploads on s_up and downloads on s_down, ordered against the
-  // kernels on `stream` by events, so that the copies of one call overlap the
-  // kernels of another when the plane is called from several threads. The
-  // lock is held while a call is queued; the caller then waits on its own
-  // completion event.
+  // Host path (fft3d_plane_filter, fft3d_plane_set_pattern_frame): staging
+  // sets owned by one call each until it returns (taken round robin; a call
+  // waits while all are owned), uploads on s_up and downloads on s_down,
+  // ordered against the kernels on `stream` by events, so that the copies of
+  // one call overlap the kernels of another when the plane is called from
+  // several threads. The plane's lock is held while a call is queued; the
+  // caller then waits on its own completion event.
   struct Stage {
     void* in = nullptr;
     size_t in_pitch = 0;
@@ -1535,10 +1532,6 @@ int fft3d_plane_create(const fft3d_params* p, const fft3d_plane_desc* d, int dev
         cudaEventCreateWithFlags(&sg.out_free, cudaEventDisableTiming) != cudaSuccess)
       return bail(fail(FFT3D_E_CUDA, "neo_fft3d: event creation failed"));
   }
-  P->d_in = P->stages[0].in;
-  P->in_pitch = P->stages[0].in_pitch;
-  P->d_out = P->stages[0].out;
-  P->out_pitch = P->stages[0].out_pitch;
   *out = P;
   if ((rc = fft3d_plane_reset(P))) { *out = nullptr; return bail(rc); }
   return FFT3D_OK;
@@ -1684,17 +1677,26 @@ int fft3d_plane_geometry(fft3d_plane* P, int out[8]) {
 // does from frame pframe on its first GetFrame (src/fft3d_engine.h:485-504).
 int fft3d_plane_set_pattern_frame(fft3d_plane* P, const void* src, int stride) {
   if (!P || !src) return fail(FFT3D_E_PARAM, "neo_fft3d: null argument");
+  // the upload goes through a staging set of its own (taken before the
+  // plane's lock, as the host-path calls do)
+  fft3d_plane::Stage* sg = acquire_stage(P);
+  struct Release {
+    fft3d_plane* P;
+    fft3d_plane::Stage* sg;
+    ~Release() { release_stage(P, sg); }
+  } release{P, sg};
   std::lock_guard<std::mutex> lk(P->mu);
   // pshow finds the pattern block on every frame itself (src/fft3d_engine.h:505-527)
   if (!P->pattern || P->ep.pshow) return FFT3D_OK;
   CK(cudaSetDevice(P->device), "cudaSetDevice");
-  // host-path calls still in flight may be using the first stage
+  // work already queued for the plane still reads the ring
   for (auto* st : {P->s_up, P->stream, P->s_down}) CK(cudaStreamSynchronize(st), "synchronize");
+  if (P->last_work) CK(cudaEventSynchronize(P->last_work), "synchronize");
   Slot* s = evict_slot(P, 1, 0);
   s->frame = -1;
-  CK(cudaMemcpy2DAsync(P->d_in, P->in_pitch, src, stride, (size_t)P->d.width * P->bytes, P->d.height,
+  CK(cudaMemcpy2DAsync(sg->in, sg->in_pitch, src, stride, (size_t)P->d.width * P->bytes, P->d.height,
                        cudaMemcpyHostToDevice, P->stream), "frame upload");
-  int rc = launch_forward(P, P->d_in, (long long)P->in_pitch, s->spec, P->stream);
+  int rc = launch_forward(P, sg->in, (long long)sg->in_pitch, s->spec, P->stream);
   if (rc) return rc;
   const int nb = P->g.bh * P->g.nh;
   if (P->ep.px == 0 && P->ep.py == 0) {
