@@ -87,7 +87,10 @@ int fft3d_plane_filter(fft3d_plane* h, int n, const void* const src[5], const in
 
 /* Same as fft3d_plane_filter, but src/dst are DEVICE pointers and the work is
  * queued on `stream` (a cudaStream_t; NULL = the handle's own stream) without
- * a host synchronisation. */
+ * a host synchronisation. A plane's calls are queued one at a time (its lock);
+ * their GPU work is ordered when they use one stream, as the spectrum ring and
+ * the Kalman state carry over from call to call: a caller that switches
+ * streams orders them itself (an event). */
 int fft3d_plane_filter_device(fft3d_plane* h, int n, const void* const src[5], const int src_stride[5], void* dst,
                               int dst_stride, void* stream);
 
