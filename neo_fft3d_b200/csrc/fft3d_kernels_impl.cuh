@@ -174,14 +174,20 @@ __device__ __forceinline__ void fwd_row(const ForwardArgs& a, const Win& win, in
 
 // Column c (0 < c < bw/2) forward DFT along y in place; c == 0 transforms the
 // real columns 0 and bw/2 together as one complex sequence col0 + i colN.
+// The lanes of a warp differ only in what they load and store: the FFT itself
+// is one code path for all of them (no divergent second pass).
 template <int BW, int BH>
 __device__ __forceinline__ void fwd_col(float2* Sb, int c) {
   constexpr int NH = BW / 2 + 1, HC = BW / 2;
   float2 col[BH];
-  if (c == 0) {
+  const bool dc = c == 0;
 #pragma unroll
-    for (int y = 0; y < BH; y++) col[y] = make_float2(Sb[y * NH].x, Sb[y * NH + HC].x);
-    cfft<BH, -1>(col);
+  for (int y = 0; y < BH; y++) {
+    const float2 v = Sb[y * NH + c];
+    col[y] = dc ? make_float2(v.x, Sb[y * NH + HC].x) : v;
+  }
+  cfft<BH, -1>(col);
+  if (dc) {
 #pragma unroll
     for (int h = 0; h < BH; h++) {
       const float2 zh = col[h], zm = cconj(col[(BH - h) % BH]);
@@ -190,9 +196,6 @@ __device__ __forceinline__ void fwd_col(float2* Sb, int c) {
       Sb[h * NH + HC] = make_float2(0.5f * d.y, -0.5f * d.x);
     }
   } else {
-#pragma unroll
-    for (int y = 0; y < BH; y++) col[y] = Sb[y * NH + c];
-    cfft<BH, -1>(col);
 #pragma unroll
     for (int h = 0; h < BH; h++) Sb[h * NH + c] = col[h];
   }
@@ -204,22 +207,25 @@ template <int BW, int BH>
 __device__ __forceinline__ void inv_col(float2* Sb, int c) {
   constexpr int NH = BW / 2 + 1, HC = BW / 2;
   float2 col[BH];
-  if (c == 0) {
+  const bool dc = c == 0;
 #pragma unroll
-    for (int h = 0; h < BH; h++) {
-      const float2 x0 = Sb[h * NH], xn = Sb[h * NH + HC];
+  for (int h = 0; h < BH; h++) {
+    const float2 x0 = Sb[h * NH + c];
+    if (dc) {
+      const float2 xn = Sb[h * NH + HC];
       col[h] = make_float2(x0.x - xn.y, x0.y + xn.x);  // x0 + i xn
+    } else {
+      col[h] = x0;
     }
-    cfft<BH, +1>(col);
+  }
+  cfft<BH, +1>(col);
+  if (dc) {
 #pragma unroll
     for (int y = 0; y < BH; y++) {
       Sb[y * NH] = make_float2(col[y].x, 0.f);
       Sb[y * NH + HC] = make_float2(col[y].y, 0.f);
     }
   } else {
-#pragma unroll
-    for (int h = 0; h < BH; h++) col[h] = Sb[h * NH + c];
-    cfft<BH, +1>(col);
 #pragma unroll
     for (int y = 0; y < BH; y++) Sb[y * NH + c] = col[y];
   }
@@ -323,7 +329,7 @@ __device__ __forceinline__ void forward_cta(const ForwardArgs& a, int cta) {
 }
 
 template <int BW, int BH, typename T>
-__global__ void __launch_bounds__(kWarps * 32) k_forward(ForwardArgs a) {
+__global__ void __launch_bounds__(kWarps * 32, 5) k_forward(ForwardArgs a) {
   forward_cta<BW, BH, T>(a, blockIdx.x);
 }
 
@@ -331,7 +337,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_forward(ForwardArgs a) {
 // x % fs.ctas of frame x / fs.ctas (one launch instead of one per frame, so
 // the grid has no per-frame wave tail).
 template <int BW, int BH, typename T>
-__global__ void __launch_bounds__(kWarps * 32) k_forward_frames(ForwardArgs a, FwdFrameSet fs) {
+__global__ void __launch_bounds__(kWarps * 32, 5) k_forward_frames(ForwardArgs a, FwdFrameSet fs) {
   const int j = blockIdx.x / fs.ctas, c = blockIdx.x - j * fs.ctas;
   FrameFwd w{nullptr, 0, nullptr};
 #pragma unroll
