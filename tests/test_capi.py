@@ -74,3 +74,21 @@ def test_batch_argument_checks_without_gpu():
     assert rc in (0, -6)
     if rc == 0:
         L.fft3d_batch_destroy(h)
+
+
+def test_frame_group_and_timing_argument_checks_without_gpu():
+    """Frame-group calls and the batch timing counters refuse bad arguments
+    before any CUDA call."""
+    L = engine.lib()
+    p = (ctypes.c_void_p * 20)()
+    s = (ctypes.c_int * 20)()
+    d = (ctypes.c_void_p * 16)()
+    ds = (ctypes.c_int * 16)()
+    for fn in (lambda c: L.fft3d_plane_filter_frames_device(None, 0, c, p, s, d, ds, None),
+               lambda c: L.fft3d_plane_filter_frames(None, 0, c, p, s, d, ds)):
+        for count in (0, 4, 17):
+            assert fn(count) == -1
+            assert "frame group" in L.fft3d_last_error().decode()
+    out = (ctypes.c_double * 12)()
+    assert L.fft3d_batch_timing(None, out) == -1
+    assert L.fft3d_batch_set_timing(None, 1) == -1
