@@ -143,8 +143,8 @@ struct fft3d_plane {
   Stage stages[kStages];
   std::condition_variable stage_cv;  // with pool_mu: a stage became free
   // Host frame groups (fft3d_plane_filter_frames): per call, the group's
-  // uploaded frames and its outputs in pitched device planes (grown to the
-  // largest group), used round robin like the one-frame stages.
+  // uploaded frames and its outputs in device planes (grown to the largest
+  // group), exclusive to one call until it returns, like the one-frame stages.
   struct GroupStage {
     // planes of `row` bytes per line, no padding, one after another: frames
     // that are contiguous in host memory move in one copy
@@ -154,10 +154,12 @@ struct fft3d_plane {
     cudaEvent_t in_free = nullptr;   // the kernels reading `in` are done
     cudaEvent_t out_free = nullptr;  // the downloads of `out` are done
     int* h_flags = nullptr;          // pinned copy of the device error flag
+    bool busy = false;               // owned by a call (gstage_cv)
   };
   static constexpr int kGroupStages = 4;
   GroupStage gstages[kGroupStages];
   int next_gstage = 0;
+  std::condition_variable gstage_cv;  // with pool_mu: a group stage became free
   int next_stage = 0;
   Stage* cur = nullptr;            // the stage of the call being queued
   cudaEvent_t call_done = nullptr;  // completion event of the call being queued
@@ -1202,6 +1204,38 @@ int group_stage_size(fft3d_plane* P, fft3d_plane::GroupStage* gs, int nin, int n
   return FFT3D_OK;
 }
 
+// A group stage for one host frame-group call, exclusive until the call
+// returns: its pinned error flag is read after the call's wait, so no other
+// call may reset it meanwhile (a call waits while all stages are owned).
+struct GroupStageLease {
+  fft3d_plane* P;
+  fft3d_plane::GroupStage* gs = nullptr;
+  explicit GroupStageLease(fft3d_plane* p) : P(p) {
+    std::unique_lock<std::mutex> lk(P->pool_mu);
+    for (;;) {
+      for (int k = 0; k < fft3d_plane::kGroupStages; k++) {
+        const int i = (P->next_gstage + k) % fft3d_plane::kGroupStages;
+        if (!P->gstages[i].busy) {
+          gs = &P->gstages[i];
+          gs->busy = true;
+          P->next_gstage = (i + 1) % fft3d_plane::kGroupStages;
+          return;
+        }
+      }
+      P->gstage_cv.wait(lk);
+    }
+  }
+  ~GroupStageLease() {
+    {
+      std::lock_guard<std::mutex> lk(P->pool_mu);
+      gs->busy = false;
+    }
+    P->gstage_cv.notify_one();
+  }
+  GroupStageLease(const GroupStageLease&) = delete;
+  GroupStageLease& operator=(const GroupStageLease&) = delete;
+};
+
 // Host frame group: the frames the group needs and the ring lacks go up on
 // the upload stream into the stage's planes, the group runs on the plane's
 // stream, and its outputs come down on the download stream; the plane's
@@ -1209,13 +1243,12 @@ int group_stage_size(fft3d_plane* P, fft3d_plane::GroupStage* gs, int nin, int n
 int filter_group_host(fft3d_plane* P, int n0, int count, const void* const* src, const int* src_stride,
                       void* const* dst, const int* dst_stride) {
   cudaEvent_t done = nullptr;
-  fft3d_plane::GroupStage* gs = nullptr;
+  GroupStageLease lease(P);
+  fft3d_plane::GroupStage* gs = lease.gs;
   {
     std::lock_guard<std::mutex> lk(P->mu);
     CK(cudaSetDevice(P->device), "cudaSetDevice");
     cudaStream_t st = P->stream;
-    gs = &P->gstages[P->next_gstage];
-    P->next_gstage = (P->next_gstage + 1) % fft3d_plane::kGroupStages;
     int rc = group_stage_size(P, gs, count + 4, count);
     if (rc) return rc;
     const size_t row = (size_t)P->d.width * P->bytes;

@@ -202,9 +202,12 @@ def test_host_frame_groups_match_per_frame(gpu, name):
 
 
 @pytest.mark.gpu
-def test_host_frame_groups_from_threads(gpu):
+@pytest.mark.parametrize("threads,group", [(4, 4), (7, 2)])
+def test_host_frame_groups_from_threads(gpu, threads, group):
     """Several host threads taking groups of one plane from a shared counter
-    (as the bench's end-to-end arm does): the outputs equal a serial run."""
+    (as the bench's end-to-end arm does): the outputs equal a serial run.
+    Seven threads outnumber the plane's four group staging sets, so calls
+    wait for a free set."""
     import threading
     clip, filt = CASES[0][1], CASES[0][2]
     planes = synth.make_clip(frames=F, noise_sigma=5.0, **clip)
@@ -218,14 +221,14 @@ def test_host_frame_groups_from_threads(gpu):
             while True:
                 with lock:
                     n0 = counter[0]
-                    counter[0] += 4
+                    counter[0] += group
                 if n0 >= F:
                     return
-                k = min(4, F - n0)
+                k = min(group, F - n0)
                 e.filter_frames(n0, [a[n] if 0 <= n < F else None for n in range(n0 - 2, n0 + k + 2)],
                                 [o[n] for n in range(n0, n0 + k)])
 
-        th = [threading.Thread(target=work) for _ in range(4)]
+        th = [threading.Thread(target=work) for _ in range(threads)]
         for t in th:
             t.start()
         for t in th:
