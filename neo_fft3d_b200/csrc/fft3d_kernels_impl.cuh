@@ -365,14 +365,29 @@ __global__ void __launch_bounds__(kWarps * 32) k_forward_batch(const ForwardArgs
 
 // ---------------------------------------------------------------- filters
 
-__device__ __forceinline__ float sharpen_fact(const InverseArgs& a, float psd, int bin) {
-  // src/code_impl/Apply.cpp:129-131
-  return 1.f + a.c.sharpen * __ldg(a.t.wsharpen + bin) *
-                   sqrtf(__fdividef(psd * a.c.smax2n, (psd + a.c.smin2n) * (psd + a.c.smax2n)));
+// The per-bin table values one bin's filter reads (the same for every
+// block). Loaded before the filter arithmetic, so that their latency is
+// hidden behind it instead of stalling the first use.
+struct BinTab {
+  float2 grid;  // gridsample, when degrid != 0
+  float wsh;    // sharpen weight, when sharpen != 0
+  float wdh;    // dehalo weight, when dehalo != 0
+};
+__device__ __forceinline__ BinTab bin_tab(const InverseArgs& a, int bin) {
+  BinTab t{make_float2(0.f, 0.f), 0.f, 0.f};
+  if (a.c.degrid != 0.f) t.grid = __ldg(a.t.grid + bin);
+  if (a.c.use_sharpen) t.wsh = __ldg(a.t.wsharpen + bin);
+  if (a.c.use_dehalo) t.wdh = __ldg(a.t.wdehalo + bin);
+  return t;
 }
-__device__ __forceinline__ float dehalo_fact(const InverseArgs& a, float psd, int bin) {
+
+__device__ __forceinline__ float sharpen_fact(const InverseArgs& a, float psd, float wsh) {
+  // src/code_impl/Apply.cpp:129-131
+  return 1.f + a.c.sharpen * wsh * sqrtf(__fdividef(psd * a.c.smax2n, (psd + a.c.smin2n) * (psd + a.c.smax2n)));
+}
+__device__ __forceinline__ float dehalo_fact(const InverseArgs& a, float psd, float wdh) {
   // src/code_impl/Apply.cpp:132
-  return __fdividef(psd + a.c.ht2n, (psd + a.c.ht2n) + a.c.dehalo * __ldg(a.t.wdehalo + bin) * psd);
+  return __fdividef(psd + a.c.ht2n, (psd + a.c.ht2n) + a.c.dehalo * wdh * psd);
 }
 
 // limited Wiener factor applied to one temporal component, code_impl_C.h:34-40
@@ -395,7 +410,7 @@ __device__ __forceinline__ float learned_noise(const InverseArgs& a, size_t off,
 // 0 = Kalman (updates the state when `commit`), -1 = sharpen only (identity).
 template <int MODE>
 __device__ __forceinline__ float2 filter_vals(const InverseArgs& a, const float2 (&w)[5], size_t off, int bin, float gf,
-                                              bool commit) {
+                                              const BinTab& tb, bool commit) {
   const float2 cur = w[2];
   if constexpr (MODE == MODE_SHARPEN_ONLY) {
     return cur;
@@ -437,19 +452,16 @@ __device__ __forceinline__ float2 filter_vals(const InverseArgs& a, const float2
   } else if constexpr (MODE == MODE_WIENER2D) {
     // src/code_impl/Apply.cpp:13-65
     float2 gc = make_float2(0.f, 0.f);
-    if (a.c.degrid != 0.f) {
-      const float2 gs = __ldg(a.t.grid + bin);
-      gc = make_float2(gf * gs.x, gf * gs.y);
-    }
+    if (a.c.degrid != 0.f) gc = make_float2(gf * tb.grid.x, gf * tb.grid.y);
     const float cr = cur.x - gc.x, ci = cur.y - gc.y;
     const float psd = cr * cr + ci * ci + 1e-15f;
     const float noise = a.psd ? learned_noise(a, off, bin) : a.c.pattern ? __ldg(a.t.pattern2d + bin) : a.c.sigma2n;
     const float q = __fdividef(psd - noise, psd);
     float f = q > a.c.lowlimit ? q : a.c.lowlimit;
     if (a.c.fuse_sharpen) {
-      if (a.c.use_sharpen && a.c.use_dehalo) f *= sharpen_fact(a, psd, bin) * dehalo_fact(a, psd, bin);
-      else if (a.c.use_sharpen) f *= sharpen_fact(a, psd, bin);
-      else if (a.c.use_dehalo) f *= dehalo_fact(a, psd, bin);
+      if (a.c.use_sharpen && a.c.use_dehalo) f *= sharpen_fact(a, psd, tb.wsh) * dehalo_fact(a, psd, tb.wdh);
+      else if (a.c.use_sharpen) f *= sharpen_fact(a, psd, tb.wsh);
+      else if (a.c.use_dehalo) f *= dehalo_fact(a, psd, tb.wdh);
     }
     return make_float2(cr * f + gc.x, ci * f + gc.y);
   } else {
@@ -457,9 +469,8 @@ __device__ __forceinline__ float2 filter_vals(const InverseArgs& a, const float2
     constexpr float kb = (float)MODE;
     float g0 = 0.f, g1 = 0.f;
     if (a.c.degrid != 0.f) {
-      const float2 gs = __ldg(a.t.grid + bin);
-      g0 = gf * gs.x * kb;
-      g1 = gf * gs.y * kb;
+      g0 = gf * tb.grid.x * kb;
+      g1 = gf * tb.grid.y * kb;
     }
     const float noise = a.psd ? learned_noise(a, off, bin) : a.c.pattern ? __ldg(a.t.pattern3d + bin) : a.c.sigma2n;
     const float ll = a.c.lowlimit;
@@ -538,22 +549,19 @@ __device__ __forceinline__ float2 filter_bin(const InverseArgs& a, size_t off, i
 #pragma unroll
   for (int k = 0; k < 5; k++)
     w[k] = (k >= win_lo<MODE>() && k <= win_hi<MODE>()) ? __ldg(a.in[k] + off + bin) : make_float2(0.f, 0.f);
-  return filter_vals<MODE>(a, w, off, bin, gf, commit);
+  return filter_vals<MODE>(a, w, off, bin, gf, bin_tab(a, bin), commit);
 }
 
 // separate sharpen/dehalo pass on a filtered bin, src/code_impl/Sharpen.cpp:13-63
-__device__ __forceinline__ float2 sharpen_bin(const InverseArgs& a, float2 v, int bin, float gf) {
+__device__ __forceinline__ float2 sharpen_bin(const InverseArgs& a, float2 v, const BinTab& tb, float gf) {
   float2 gc = make_float2(0.f, 0.f);
-  if (a.c.degrid != 0.f) {
-    const float2 gs = __ldg(a.t.grid + bin);
-    gc = make_float2(gf * gs.x, gf * gs.y);
-  }
+  if (a.c.degrid != 0.f) gc = make_float2(gf * tb.grid.x, gf * tb.grid.y);
   const float cr = v.x - gc.x, ci = v.y - gc.y;
   const float psd = cr * cr + ci * ci + 1.0e-15f;
   float f;
-  if (a.c.use_sharpen && a.c.use_dehalo) f = sharpen_fact(a, psd, bin) * dehalo_fact(a, psd, bin);
-  else if (a.c.use_sharpen) f = sharpen_fact(a, psd, bin);
-  else f = dehalo_fact(a, psd, bin);
+  if (a.c.use_sharpen && a.c.use_dehalo) f = sharpen_fact(a, psd, tb.wsh) * dehalo_fact(a, psd, tb.wdh);
+  else if (a.c.use_sharpen) f = sharpen_fact(a, psd, tb.wsh);
+  else f = dehalo_fact(a, psd, tb.wdh);
   return make_float2(cr * f + gc.x, ci * f + gc.y);
 }
 
@@ -585,8 +593,8 @@ __global__ void __launch_bounds__(256) k_filter_bins(InverseArgs a, float2* F, i
       w0[k] = in ? make_float2(wv[k - LO].x, wv[k - LO].y) : make_float2(0.f, 0.f);
       w1[k] = in ? make_float2(wv[k - LO].z, wv[k - LO].w) : make_float2(0.f, 0.f);
     }
-    const float2 v0 = filter_vals<MODE>(a, w0, off, bin, gf, true);
-    const float2 v1 = filter_vals<MODE>(a, w1, off, bin + 1, gf, true);
+    const float2 v0 = filter_vals<MODE>(a, w0, off, bin, gf, bin_tab(a, bin), true);
+    const float2 v1 = filter_vals<MODE>(a, w1, off, bin + 1, gf, bin_tab(a, bin + 1), true);
     reinterpret_cast<float4*>(F)[q] = make_float4(v0.x, v0.y, v1.x, v1.y);
   }
 }
@@ -617,12 +625,17 @@ __device__ __forceinline__ float2 ld_stream(const float2* p) {
 // Where a CTA finds its window spectra and writes its time-domain blocks:
 // the launch arguments (one output frame per launch), or pointers picked for
 // one frame of a frame group (k_filter_inverse_frames).
+// kHoistTab: a chunk's per-bin table values are loaded before its filter
+// arithmetic (measured faster one frame per launch); the frame-group kernel
+// loads each next to its first use (faster there: fewer live registers).
 struct ArgsWin {
+  static constexpr bool kHoistTab = true;
   const InverseArgs& a;
   __device__ __forceinline__ const float2* in(int k) const { return a.in[k]; }
   __device__ __forceinline__ float* tdom() const { return a.tdom; }
 };
 struct FrameWin {
+  static constexpr bool kHoistTab = false;
   const float2* p[5];
   float* t;
   __device__ __forceinline__ const float2* in(int k) const { return p[k]; }
@@ -684,13 +697,26 @@ __device__ __forceinline__ void filter_inverse_cta_w(const InverseArgs& a, int v
 #pragma unroll
       for (int k = 0; k < 5; k++) w[k] = (k >= LO && k < LO + NG) ? buf[j % D][k - LO] : make_float2(0.f, 0.f);
       if (NEWEST_IN_S && i < BINS) w[HI] = S[b * BINS + i];
+      BinTab tb{make_float2(0.f, 0.f), 0.f, 0.f};
+      if constexpr (Win::kHoistTab) {
+        // the chunk's table values first: the filter arithmetic hides their latency
+        if (i < BINS) tb = bin_tab(a, i);
+      } else if (MODE == MODE_WIENER2D && a.c.fuse_sharpen) {
+        if (i < BINS) tb = bin_tab(a, i);  // the Wiener factor takes the sharpen/dehalo weights
+      } else {
+        if (i < BINS && a.c.degrid != 0.f) tb.grid = __ldg(a.t.grid + i);
+      }
       if (NG > 0 && j + D < PER) load(j + D, buf[j % D]);
       float2 v = make_float2(0.f, 0.f);
-      if (i < BINS) v = filter_vals<MODE>(a, w, off, i, gf, true);
+      if (i < BINS) v = filter_vals<MODE>(a, w, off, i, gf, tb, true);
       if (a.c.do_sharpen) {
         // grid fraction of the sharpen pass: the filtered DC (lane 0, chunk 0)
         if (j == 0) gsh = a.c.degrid * __shfl_sync(0xffffffffu, v.x, 0) / gs0;
-        if (i < BINS) v = sharpen_bin(a, v, i, gsh);
+        if constexpr (!Win::kHoistTab) {
+          if (i < BINS && a.c.use_sharpen) tb.wsh = __ldg(a.t.wsharpen + i);
+          if (i < BINS && a.c.use_dehalo) tb.wdh = __ldg(a.t.wdehalo + i);
+        }
+        if (i < BINS) v = sharpen_bin(a, v, tb, gsh);
       }
       if (i < BINS) S[b * BINS + i] = v;
     }
@@ -850,16 +876,18 @@ __global__ void __launch_bounds__(kBulkWarps * 32) k_filter_inverse_bulk(Inverse
     for (int j = 0; j < PER; j++) {
       const int i = lane + 32 * j;
       float2 v = make_float2(0.f, 0.f);
+      BinTab tb{make_float2(0.f, 0.f), 0.f, 0.f};
       if (i < BINS) {
+        tb = bin_tab(a, i);
         float2 w[5];
 #pragma unroll
         for (int k = 0; k < 5; k++)
           w[k] = (k >= LO && k < LO + NW) ? stage[(k - LO) * BINS + i] : make_float2(0.f, 0.f);
-        v = filter_vals<MODE>(a, w, off, i, gf, true);
+        v = filter_vals<MODE>(a, w, off, i, gf, tb, true);
       }
       if (a.c.do_sharpen) {
         if (j == 0) gsh = a.c.degrid * __shfl_sync(0xffffffffu, v.x, 0) / gs0;
-        if (i < BINS) v = sharpen_bin(a, v, i, gsh);
+        if (i < BINS) v = sharpen_bin(a, v, tb, gsh);
       }
       if (i < BINS) S[i] = v;
     }
