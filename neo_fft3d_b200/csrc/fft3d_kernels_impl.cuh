@@ -373,11 +373,16 @@ struct BinTab {
   float wsh;    // sharpen weight, when sharpen != 0
   float wdh;    // dehalo weight, when dehalo != 0
 };
+// Only the values that MODE's filter and the sharpen pass read are loaded
+// (Kalman and sharpen-only read the grid only in a sharpen pass; the weights
+// are read by a sharpen pass or by Wiener 2D's fused factor).
+template <int MODE>
 __device__ __forceinline__ BinTab bin_tab(const InverseArgs& a, int bin) {
   BinTab t{make_float2(0.f, 0.f), 0.f, 0.f};
-  if (a.c.degrid != 0.f) t.grid = __ldg(a.t.grid + bin);
-  if (a.c.use_sharpen) t.wsh = __ldg(a.t.wsharpen + bin);
-  if (a.c.use_dehalo) t.wdh = __ldg(a.t.wdehalo + bin);
+  const bool sh = a.c.do_sharpen || (MODE == MODE_WIENER2D && a.c.fuse_sharpen);
+  if (a.c.degrid != 0.f && (MODE >= 1 || a.c.do_sharpen)) t.grid = __ldg(a.t.grid + bin);
+  if (sh && a.c.use_sharpen) t.wsh = __ldg(a.t.wsharpen + bin);
+  if (sh && a.c.use_dehalo) t.wdh = __ldg(a.t.wdehalo + bin);
   return t;
 }
 
@@ -549,7 +554,7 @@ __device__ __forceinline__ float2 filter_bin(const InverseArgs& a, size_t off, i
 #pragma unroll
   for (int k = 0; k < 5; k++)
     w[k] = (k >= win_lo<MODE>() && k <= win_hi<MODE>()) ? __ldg(a.in[k] + off + bin) : make_float2(0.f, 0.f);
-  return filter_vals<MODE>(a, w, off, bin, gf, bin_tab(a, bin), commit);
+  return filter_vals<MODE>(a, w, off, bin, gf, bin_tab<MODE>(a, bin), commit);
 }
 
 // separate sharpen/dehalo pass on a filtered bin, src/code_impl/Sharpen.cpp:13-63
@@ -593,8 +598,8 @@ __global__ void __launch_bounds__(256) k_filter_bins(InverseArgs a, float2* F, i
       w0[k] = in ? make_float2(wv[k - LO].x, wv[k - LO].y) : make_float2(0.f, 0.f);
       w1[k] = in ? make_float2(wv[k - LO].z, wv[k - LO].w) : make_float2(0.f, 0.f);
     }
-    const float2 v0 = filter_vals<MODE>(a, w0, off, bin, gf, bin_tab(a, bin), true);
-    const float2 v1 = filter_vals<MODE>(a, w1, off, bin + 1, gf, bin_tab(a, bin + 1), true);
+    const float2 v0 = filter_vals<MODE>(a, w0, off, bin, gf, bin_tab<MODE>(a, bin), true);
+    const float2 v1 = filter_vals<MODE>(a, w1, off, bin + 1, gf, bin_tab<MODE>(a, bin + 1), true);
     reinterpret_cast<float4*>(F)[q] = make_float4(v0.x, v0.y, v1.x, v1.y);
   }
 }
@@ -700,9 +705,9 @@ __device__ __forceinline__ void filter_inverse_cta_w(const InverseArgs& a, int v
       BinTab tb{make_float2(0.f, 0.f), 0.f, 0.f};
       if constexpr (Win::kHoistTab) {
         // the chunk's table values first: the filter arithmetic hides their latency
-        if (i < BINS) tb = bin_tab(a, i);
+        if (i < BINS) tb = bin_tab<MODE>(a, i);
       } else if (MODE == MODE_WIENER2D && a.c.fuse_sharpen) {
-        if (i < BINS) tb = bin_tab(a, i);  // the Wiener factor takes the sharpen/dehalo weights
+        if (i < BINS) tb = bin_tab<MODE>(a, i);  // the Wiener factor takes the sharpen/dehalo weights
       } else {
         if (i < BINS && a.c.degrid != 0.f) tb.grid = __ldg(a.t.grid + i);
       }
@@ -878,7 +883,7 @@ __global__ void __launch_bounds__(kBulkWarps * 32) k_filter_inverse_bulk(Inverse
       float2 v = make_float2(0.f, 0.f);
       BinTab tb{make_float2(0.f, 0.f), 0.f, 0.f};
       if (i < BINS) {
-        tb = bin_tab(a, i);
+        tb = bin_tab<MODE>(a, i);
         float2 w[5];
 #pragma unroll
         for (int k = 0; k < 5; k++)
