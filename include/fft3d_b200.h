@@ -121,8 +121,10 @@ int fft3d_plane_filter_frames_device(fft3d_plane* h, int n0, int count, const vo
  * fft3d_plane_filter): the frames the group needs and the device does not
  * hold are uploaded, the outputs downloaded, and the call returns when they
  * are in dst. Calls from several threads overlap one call's copies with
- * another's kernels. Planes with crop borders, and planes that are not
- * grouped, go through fft3d_plane_filter frame by frame. */
+ * another's kernels; each call owns one of the plane's 4 group staging sets
+ * until it returns (a fifth concurrent call waits for a free one). Planes
+ * with crop borders, and planes that are not grouped, go through
+ * fft3d_plane_filter frame by frame. */
 int fft3d_plane_filter_frames(fft3d_plane* h, int n0, int count, const void* const* src, const int* src_stride,
                               void* const* dst, const int* dst_stride);
 
