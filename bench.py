@@ -34,6 +34,7 @@ on the data path ("scaling": "weak").
 from __future__ import annotations
 
 import argparse
+import faulthandler
 import json
 import os
 import statistics
@@ -134,48 +135,91 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def run_reference(clip_kw, filt, frames, threads, first=10):
-    """Reference plugin (oracle/_ref) rendering `frames` output frames with
-    `threads` host threads, opt=0 (its SIMD path), ncpu=1. Returns seconds."""
+# The reference plugin grows its per-thread scratch and its spectrum cache the
+# first time more threads call it at once than before (src/fft3d_engine.h:
+# 460-483): cache::resize appends to the cache's LRU list under
+# thread_check_mutex while other threads reorder that list under cache_mutex
+# (src/cache.hpp:34-71, src/fft3d_engine.h:647-667), and the scratch vectors
+# it appends to are indexed after the lock is released (:481-483). That race
+# can corrupt the heap while the thread count ramps up, so the reference is
+# timed in a child process of its own: one filter node per process (as one
+# script renders a clip), the ramp-up inside an untimed first render, and a
+# fresh child if one dies by a signal.
+REF_FIRST, REF_LAST = 10, 110  # frames rendered by the reference arm (the clip has 120)
+
+
+def reference_child(args):
+    """Child-process body of the reference measurement: one reference filter
+    node over the 1080p bt=5 clip, an untimed ramp-up render of `threads`
+    frames, then args.warmup untimed and args.steps timed renders of `frames`
+    frames each (consecutive frame ranges, wrapping within the clip). Prints
+    one JSON line with the per-step seconds."""
     from oracle import reference
-    planes = clip_kw["planes"]
+    clip_kw, filt = workload()
+    planes = synth.make_clip(**clip_kw)
+    threads = args.ref_threads or os.cpu_count() or 1
     c = reference.core()
     clip = c.clip(planes)
     node = c.invoke("neo_fft3d", "FFT3D", clip, opt=0, ncpu=1, **filt)
+    span = REF_LAST - REF_FIRST
     t = time.perf_counter()
-    node.render(first=first, count=frames, threads=threads)
-    secs = time.perf_counter() - t
-    del node, clip  # frees the reference's engines and spectrum caches
-    import gc
-    gc.collect()
-    return secs
+    node.render(first=REF_FIRST, count=threads, threads=threads)
+    per_frame = (time.perf_counter() - t) / threads
+    frames = args.ref_frames or int(max(1, min(span, args.ref_budget / max(1, args.steps + args.warmup) / per_frame)))
+    frames = min(frames, span)
+    start = REF_FIRST + threads
+    secs = []
+    for i in range(args.warmup + args.steps):
+        if start + frames > REF_LAST:
+            start = REF_FIRST
+        t = time.perf_counter()
+        node.render(first=start, count=frames, threads=threads)
+        if i >= args.warmup:
+            secs.append(time.perf_counter() - t)
+        start += frames
+    print(json.dumps({"frames": frames, "threads": threads, "secs": secs, "ramp_up_s_per_frame": per_frame}),
+          flush=True)
+
+
+def run_reference_isolated(steps, warmup, frames=0, budget=150.0, threads=0, attempts=3):
+    """reference_child in a fresh process (retried when a child dies by a
+    signal); returns its result dict plus the number of attempts."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--ref-child",
+           "--steps", str(steps), "--warmup", str(warmup), "--ref-frames", str(frames),
+           "--ref-budget", str(budget), "--ref-threads", str(threads)]
+    env = dict(os.environ)
+    env.pop("RANK", None)
+    env.pop("WORLD_SIZE", None)
+    err = ""
+    for k in range(attempts):
+        r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True, env=env)
+        lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+        if r.returncode == 0 and lines:
+            out = json.loads(lines[-1])
+            out["attempts"] = k + 1
+            return out
+        err = f"child rc {r.returncode}: {r.stderr.strip()[-300:]}"
+        if r.returncode >= 0:
+            break  # an error, not a crash: no retry
+    raise RuntimeError(err)
 
 
 def reference_arm(args, rank):
-    clip_kw, filt = workload()
     if rank != 0:
         return None
-    planes = synth.make_clip(**clip_kw)
-    threads = os.cpu_count() or 1
-    # size the per-step sample so that the whole run stays within ~3 minutes
-    t1 = run_reference({"planes": planes}, filt, threads, threads)
-    per_frame = t1 / threads
-    budget = 150.0
-    frames = int(max(1, min(clip_kw["frames"] - 20, budget / max(1, args.steps + args.warmup) / per_frame)))
-    for _ in range(args.warmup):
-        run_reference({"planes": planes}, filt, frames, threads)
-    total = 0.0
-    for _ in range(args.steps):
-        total += run_reference({"planes": planes}, filt, frames, threads)
-    fps = args.steps * frames / total
+    r = run_reference_isolated(args.steps, args.warmup)
+    frames, threads, secs = r["frames"], r["threads"], r["secs"]
+    total = sum(secs)
+    fps = len(secs) * frames / total
     line = {
         "impl": "reference", "metric": METRIC, "value": fps, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / len(secs),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "frames_per_step": frames, "opt": 0, "ncpu": 1, "host_threads": threads},
+        "config": {"workload": WORKLOAD, "frames_per_step": frames, "opt": 0, "ncpu": 1, "host_threads": threads,
+                   "child_attempts": r["attempts"]},
         "cpu_baseline": {"value": fps, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": f"{frames} output frames (of 120) of the 1080p bt=5 clip per step, "
-                                   f"{threads} host threads (frame-parallel), opt=0, FFT = project FFTW-API shim"},
+                         "sample": f"{frames} output frames (of 120) of the 1080p bt=5 clip per step, one filter "
+                                   f"node, {threads} host threads (frame-parallel), opt=0, FFT = project FFTW-API shim"},
         "e2e": {"value": fps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     return line
@@ -262,6 +306,7 @@ def kalman_4k(args, torch, dist, engine, make_params, plane_descs, local, world,
 
 
 def main():
+    faulthandler.enable()  # a native fault leaves its Python stack on stderr
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
@@ -270,9 +315,17 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-kalman", action="store_true")
+    # child process of the reference measurement (run_reference_isolated)
+    ap.add_argument("--ref-child", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--ref-frames", type=int, default=0, help=argparse.SUPPRESS)
+    ap.add_argument("--ref-budget", type=float, default=150.0, help=argparse.SUPPRESS)
+    ap.add_argument("--ref-threads", type=int, default=0, help=argparse.SUPPRESS)
     ap.add_argument("--arms", default=",".join(PATHS),
                     help="comma-separated subset of the timed arms (profiling runs); the comparisons need all")
     args = ap.parse_args()
+    if args.impl == "reference" and args.ref_child:
+        reference_child(args)  # warm-up count as given (the ramp-up render is untimed anyway)
+        return
     args.warmup = max(args.warmup, 3)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -529,13 +582,16 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # in a child process (see reference_child): the reference cannot take
+        # this process and its GPU record down with it
         try:
             threads = os.cpu_count() or 1
-            sample = 2 * threads
-            secs = run_reference({"planes": planes}, filt, sample, threads)
-            cpu = {"value": sample / secs, "unit": UNIT, "cores": threads, "kind": "reference",
-                   "sample": f"{sample} output frames (frames 10..{10 + sample - 1}) of the same clip, "
-                             f"{threads} host threads, opt=0, ncpu=1, FFT = project FFTW-API shim"}
+            r = run_reference_isolated(steps=1, warmup=0, frames=2 * threads, threads=threads)
+            sample, secs = r["frames"], sum(r["secs"])
+            cpu = {"value": sample / secs, "unit": UNIT, "cores": r["threads"], "kind": "reference",
+                   "sample": f"{sample} output frames of the same clip after a ramp-up render of {threads}, "
+                             f"one filter node, {r['threads']} host threads, opt=0, ncpu=1, "
+                             f"FFT = project FFTW-API shim (child attempts: {r['attempts']})"}
         except Exception as ex:  # the reference build is optional on a box
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {ex}"}
 

@@ -184,8 +184,12 @@ int fft3d_plane_timing(fft3d_plane* h, double out[15]);
  * previous call's contents in it (each call writes everything it reads), so
  * calls whose GPU work overlaps race: keep them on one stream. The first call
  * on a device resolves the array's address and uploads the FFT twiddle tables;
- * make it before any stream capture. Output matches fft3d_plane_filter_device
- * with the same parameters. */
+ * make it before any stream capture. Later calls only queue kernels on
+ * `stream` (the plane's tables travel as kernel parameters) and never wait on
+ * it from the host. Not for use across a cudaDeviceReset of a device it has
+ * run on (the address and tables are kept per device for the process's life).
+ * Output equals fft3d_plane_filter_device's with the same parameters, byte
+ * for byte (the same kernels). */
 int fft3d_filter2d_static(const fft3d_params* p, const fft3d_plane_desc* d, const void* src, int src_stride,
                           void* dst, int dst_stride, void* stream);
 

@@ -549,7 +549,8 @@ int output_frame(fft3d_plane* P, float* tdom, const fft3d::Tables& tab, float ba
   const bool ints = P->bytes != 4;
   oa.rounder = ints ? 0.5f : 0.f;
   oa.base = base;
-  oa.maxval = P->bytes == 1 ? 255 : (1 << P->d.bits) - 1;
+  // float samples clamp to [0, 1] and have no integer maximum (no shift by 32)
+  oa.maxval = P->bytes == 1 ? 255 : (P->bytes == 2 ? (1 << P->d.bits) - 1 : 0);
   if (g_defer) {
     g_defer->ola.push_back({oa, P->bytes, g_defer->plane});
   } else {

@@ -23,7 +23,12 @@
 //    stream, or wait for one before issuing the next;
 //  * the first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress) and uploads the FFT twiddle tables; make that
-//    first call before any stream capture.
+//    first call before any stream capture. Later calls only launch kernels on
+//    the caller's stream (the plane's tables go up as kernel parameters), so
+//    they never wait on the stream from the host;
+//  * the address and the twiddle tables are kept per device number for the
+//    life of the process: do not use the call across a cudaDeviceReset of a
+//    device it has run on (they would belong to the destroyed context).
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -72,6 +77,23 @@ int static_base(int dev, void** out) {
 }
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// The plane's tables travel to the scratch array as the launch parameters of a
+// copy kernel: the launch takes them by value, so the call keeps no host
+// buffer alive, never waits on the stream from the host (a cudaMemcpyAsync
+// from pageable memory would), and the upload is ordered on the caller's
+// stream like the kernels that read it. The largest table set (48x48 blocks)
+// is 5248 floats; kernel parameters may take up to 32 KB.
+constexpr int kStaticTableFloats = 7168;
+struct StaticTableBlob {
+  float v[kStaticTableFloats];
+};
+
+// dst[0 .. n) = blob, then dst[n .. n + zeros) = 0 (the unused pattern tables)
+__global__ void k_static_tables(const __grid_constant__ StaticTableBlob b, int n, int zeros, float* dst) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + zeros; i += gridDim.x * blockDim.x)
+    dst[i] = i < n ? b.v[i] : 0.f;
+}
 
 }  // namespace
 
@@ -182,9 +204,11 @@ extern "C" int fft3d_filter2d_static(const fft3d_params* p0, const fft3d_plane_d
     return off;
   };
   const size_t o_wx = put(wx), o_wy = put(wy), o_sxl = put(sxl), o_sxr = put(sxr), o_syl = put(syl),
-               o_syr = put(syr), o_grid = put(grid), o_wsh = put(wsh), o_wdh = put(wdh),
-               o_pat = put(std::vector<float>(nb, 0.f));
-  const size_t tables_bytes = align256(blob.size() * sizeof(float));
+               o_syr = put(syr), o_grid = put(grid), o_wsh = put(wsh), o_wdh = put(wdh);
+  const size_t o_pat = blob.size();  // nb zeros, written by the table kernel
+  if (blob.size() > (size_t)kStaticTableFloats)
+    return sfail(FFT3D_E_UNSUPPORTED, "neo_fft3d: the allocation-free call's tables exceed its launch parameters");
+  const size_t tables_bytes = align256((o_pat + nb) * sizeof(float));
   const size_t spec_bytes = align256((size_t)g.nblocks * nb * sizeof(float2));
   const size_t tdom_bytes = align256((size_t)g.nblocks * bh * bw * sizeof(float));
   const size_t need = tables_bytes + spec_bytes + tdom_bytes;
@@ -200,8 +224,14 @@ extern "C" int fft3d_filter2d_static(const fft3d_params* p0, const fft3d_plane_d
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   char* B = static_cast<char*>(base);
-  err = cudaMemcpyAsync(B, blob.data(), blob.size() * sizeof(float), cudaMemcpyHostToDevice, st);
-  if (err != cudaSuccess) return sfail(FFT3D_E_CUDA, std::string("neo_fft3d: table upload: ") + cudaGetErrorString(err));
+  {
+    StaticTableBlob tb;
+    std::memcpy(tb.v, blob.data(), blob.size() * sizeof(float));
+    k_static_tables<<<8, 256, 0, st>>>(tb, (int)blob.size(), nb, reinterpret_cast<float*>(B));
+    err = cudaGetLastError();
+    if (err != cudaSuccess)
+      return sfail(FFT3D_E_CUDA, std::string("neo_fft3d: table upload: ") + cudaGetErrorString(err));
+  }
   const float* T = reinterpret_cast<const float*>(B);
   float2* spec = reinterpret_cast<float2*>(B + tables_bytes);
   float* tdom = reinterpret_cast<float*>(B + tables_bytes + spec_bytes);
@@ -266,7 +296,7 @@ extern "C" int fft3d_filter2d_static(const fft3d_params* p0, const fft3d_plane_d
   oa.norm = norm;
   oa.rounder = ints ? 0.5f : 0.f;
   oa.base = base_val;
-  oa.maxval = bytes == 1 ? 255 : (1 << d->bits) - 1;
+  oa.maxval = bytes == 1 ? 255 : (bytes == 2 ? (1 << d->bits) - 1 : 0);  // float: clamp to [0, 1]
   err = fft3d::launch_overlap_add(oa, bytes, st);
   if (err != cudaSuccess) return sfail(FFT3D_E_CUDA, std::string("neo_fft3d: overlap-add kernel: ") + cudaGetErrorString(err));
   return FFT3D_OK;
