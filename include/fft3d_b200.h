@@ -154,6 +154,30 @@ int fft3d_plane_reset(fft3d_plane* h);
 
 void fft3d_plane_destroy(fft3d_plane* h);
 
+/* Device memory this plane holds, in bytes (tables, spectrum ring, Kalman
+ * state, time-domain blocks, staging planes; frame groups grow it). No
+ * counterpart in the reference. When the environment variable
+ * NEO_FFT3D_DEVICE_ALLOC_CAP is set at fft3d_plane_create, the plane's device
+ * allocations stop at that many bytes and fail with FFT3D_E_NOMEM, as on an
+ * exhausted device (a host-side fault injection for the out-of-memory paths). */
+int fft3d_plane_device_bytes(fft3d_plane* h, uint64_t* out);
+
+/* Wait for all work queued for this plane (on any stream) and report what the
+ * device-buffer calls cannot: a bounded device-side wait of one of the
+ * plane's kernels that ran out (FFT3D_E_CUDA with "... timed out"; the flag is
+ * cleared, so the next call starts clean). Host-buffer calls report it
+ * themselves. No counterpart in the reference, whose filter runs on the host. */
+int fft3d_plane_synchronize(fft3d_plane* h);
+
+/* Test hook (host-side fault injection, no counterpart in the reference): sets
+ * the plane's device error flag to `bits`, as a kernel does when a bounded
+ * wait runs out (bit 0: tensor-core MMA completion, bit 1: bulk copy
+ * completion), after the work already queued for the plane. The next
+ * host-buffer call, or fft3d_plane_synchronize, then reports the error and
+ * clears the flag. Lets the device error path be tested without a real
+ * device fault. */
+int fft3d_plane_debug_set_error_flag(fft3d_plane* h, int bits);
+
 /* Per-kernel timing of this handle: when enabled, every launch is bracketed
  * by CUDA events on the stream it runs on. */
 int fft3d_plane_set_timing(fft3d_plane* h, int enable);

@@ -186,6 +186,10 @@ struct fft3d_plane {
   float psd_strength = 1.f;
   float* d_psd = nullptr;
   fft3d::psd::Work* psd_work = nullptr;
+  // device bytes this plane holds, and the optional cap on them
+  // (NEO_FFT3D_DEVICE_ALLOC_CAP at creation: a host-side fault injection
+  // that makes the out-of-memory paths testable; 0 = no cap)
+  size_t alloc_used = 0, alloc_cap = 0;
   bool timing = false;
   std::vector<Timed> pending;
   std::vector<cudaEvent_t> event_pool;
@@ -204,6 +208,33 @@ cudaEvent_t take_event(fft3d_plane* P) {
   cudaEvent_t e = nullptr;
   cudaEventCreate(&e);
   return e;
+}
+
+// Device allocations of a plane go through these: they count the plane's
+// bytes (fft3d_plane_device_bytes) and honour its allocation cap, failing
+// like an exhausted device would (cudaErrorMemoryAllocation).
+template <typename T>
+cudaError_t dmalloc(fft3d_plane* P, T** p, size_t bytes) {
+  if (P->alloc_cap && P->alloc_used + bytes > P->alloc_cap) return cudaErrorMemoryAllocation;
+  void* v = nullptr;
+  const cudaError_t e = cudaMalloc(&v, bytes);
+  if (e == cudaSuccess) {
+    *p = static_cast<T*>(v);
+    P->alloc_used += bytes;
+  }
+  return e;
+}
+cudaError_t dmalloc_pitch(fft3d_plane* P, void** p, size_t* pitch, size_t width, size_t height) {
+  const size_t est = ((width + 511) & ~(size_t)511) * height;  // the cap is checked on a 512-byte pitch
+  if (P->alloc_cap && P->alloc_used + est > P->alloc_cap) return cudaErrorMemoryAllocation;
+  const cudaError_t e = cudaMallocPitch(p, pitch, width, height);
+  if (e == cudaSuccess) P->alloc_used += *pitch * height;
+  return e;
+}
+void dfree(fft3d_plane* P, void* p, size_t bytes) {
+  if (!p) return;
+  cudaFree(p);
+  P->alloc_used -= std::min(bytes, P->alloc_used);
 }
 
 // Brackets one launch with events when timing is on; `bytes` is the launch's
@@ -635,7 +666,7 @@ int pshow_frame(fft3d_plane* P, int n, const void* const src[5], const int strid
   if (!P->d_pshow) {
     const int nt = P->g.bw + P->g.bh + 2 * P->g.ow + 2 * P->g.oh;
     float* t = nullptr;
-    if (cudaMalloc(&P->d_pshow, spec_bytes) != cudaSuccess || cudaMalloc(&t, nt * sizeof(float)) != cudaSuccess) {
+    if (dmalloc(P, &P->d_pshow, spec_bytes) != cudaSuccess || dmalloc(P, &t, nt * sizeof(float)) != cudaSuccess) {
       cudaGetLastError();
       return fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (pshow)");
     }
@@ -929,7 +960,7 @@ void group_range(const fft3d_plane* P, int n0, int count, int* lo, int* hi) {
 int group_resources(fft3d_plane* P, int lo, int hi, int count) {
   while ((int)P->slots.size() < hi - lo + 2) {
     Slot s;
-    if (cudaMalloc(&s.spec, P->spec_elems() * sizeof(float2)) != cudaSuccess) {
+    if (dmalloc(P, &s.spec, P->spec_elems() * sizeof(float2)) != cudaSuccess) {
       cudaGetLastError();
       return fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (spectrum ring of a frame group)");
     }
@@ -937,7 +968,7 @@ int group_resources(fft3d_plane* P, int lo, int hi, int count) {
   }
   while ((int)P->tdom_extra.size() < count - 1) {
     float* t = nullptr;
-    if (cudaMalloc(&t, (size_t)P->g.nblocks * P->g.bh * P->g.bw * sizeof(float)) != cudaSuccess) {
+    if (dmalloc(P, &t, (size_t)P->g.nblocks * P->g.bh * P->g.bw * sizeof(float)) != cudaSuccess) {
       cudaGetLastError();
       return fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (time-domain blocks of a frame group)");
     }
@@ -1182,15 +1213,19 @@ int group_stage_size(fft3d_plane* P, fft3d_plane::GroupStage* gs, int nin, int n
       cudaEventSynchronize(gs->in_free);
       cudaEventSynchronize(gs->out_free);
     }
-    cudaFree(gs->in);
-    cudaFree(gs->out);
+    dfree(P, gs->in, plane * gs->nin);
+    dfree(P, gs->out, plane * gs->nout);
     gs->in = gs->out = nullptr;
     gs->nin = gs->nout = 0;
-    if (cudaMalloc(&gs->in, plane * nin) != cudaSuccess || cudaMalloc(&gs->out, plane * nout) != cudaSuccess) {
+    if (dmalloc(P, &gs->in, plane * nin) != cudaSuccess) {
       cudaGetLastError();
       return fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (frame group staging)");
     }
     gs->nin = nin;
+    if (dmalloc(P, &gs->out, plane * nout) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (frame group staging)");
+    }
     gs->nout = nout;
   }
   if (!gs->in_free) {
@@ -1482,6 +1517,7 @@ int fft3d_plane_create(const fft3d_params* p, const fft3d_plane_desc* d, int dev
   double maxv = P->bytes == 1 ? 255.0 : (P->bytes == 2 ? (double)((1 << d->bits) - 1) : 1.0);
   gridsample(wx, wy, maxv, bw, bh, P->h_grid);
 
+  if (const char* cap = std::getenv("NEO_FFT3D_DEVICE_ALLOC_CAP")) P->alloc_cap = std::strtoull(cap, nullptr, 10);
   // device resources
   int rc = FFT3D_OK;
   auto bail = [&](int code) { free_plane(P); return code; };
@@ -1509,7 +1545,7 @@ int fft3d_plane_create(const fft3d_params* p, const fft3d_plane_desc* d, int dev
          o_syr = put(one(syr)), o_grid = put(P->h_grid), o_wsh = put(wsharpen), o_wdh = put(wdehalo),
          o_p2 = put(P->h_pattern2d), o_p3 = put(std::vector<float>(nb, 0.f));
   {
-    cudaError_t e = cudaMalloc(&P->d_tables, blob.size() * sizeof(float));
+    cudaError_t e = dmalloc(P, &P->d_tables, blob.size() * sizeof(float));
     if (e != cudaSuccess) return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (tables)"));
     e = cudaMemcpy(P->d_tables, blob.data(), blob.size() * sizeof(float), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return bail(cuda_fail(e, "table upload"));
@@ -1534,32 +1570,32 @@ int fft3d_plane_create(const fft3d_params* p, const fft3d_plane_desc* d, int dev
   int nslots = (ep.bt > 1 ? ep.bt : 1) + 2;
   P->slots.resize(nslots);
   for (auto& s : P->slots) {
-    if (cudaMalloc(&s.spec, P->spec_elems() * sizeof(float2)) != cudaSuccess)
+    if (dmalloc(P, &s.spec, P->spec_elems() * sizeof(float2)) != cudaSuccess)
       return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (spectrum ring)"));
   }
   if (P->path == 3 && ep.bw == 32 && ep.bh == 32) {
     std::vector<uint8_t> tc(fft3d::forward_tc_table_bytes());
     fft3d::forward_tc_tables(wx.data(), wy.data(), tc.data());
-    if (cudaMalloc(&P->d_tc, tc.size()) != cudaSuccess)
+    if (dmalloc(P, &P->d_tc, tc.size()) != cudaSuccess)
       return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (tensor-core tables)"));
     if (cudaMemcpy(P->d_tc, tc.data(), tc.size(), cudaMemcpyHostToDevice) != cudaSuccess)
       return bail(fail(FFT3D_E_CUDA, "neo_fft3d: tensor-core table upload failed"));
   }
-  if (cudaMalloc(&P->d_err, sizeof(int)) != cudaSuccess || cudaMemset(P->d_err, 0, sizeof(int)) != cudaSuccess)
+  if (dmalloc(P, &P->d_err, sizeof(int)) != cudaSuccess || cudaMemset(P->d_err, 0, sizeof(int)) != cudaSuccess)
     return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (error flag)"));
-  if (P->path == 0 && cudaMalloc(&P->d_filt, P->spec_elems() * sizeof(float2)) != cudaSuccess)
+  if (P->path == 0 && dmalloc(P, &P->d_filt, P->spec_elems() * sizeof(float2)) != cudaSuccess)
     return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (filtered spectrum)"));
-  if (cudaMalloc(&P->d_tdom, (size_t)g.nblocks * bh * bw * sizeof(float)) != cudaSuccess)
+  if (dmalloc(P, &P->d_tdom, (size_t)g.nblocks * bh * bw * sizeof(float)) != cudaSuccess)
     return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (time-domain blocks)"));
   if (ep.bt == 0) {  // Kalman state, :339-344
-    if (cudaMalloc(&P->d_last, P->spec_elems() * sizeof(float2)) != cudaSuccess ||
-        cudaMalloc(&P->d_cov, P->spec_elems() * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&P->d_covp, P->spec_elems() * sizeof(float)) != cudaSuccess)
+    if (dmalloc(P, &P->d_last, P->spec_elems() * sizeof(float2)) != cudaSuccess ||
+        dmalloc(P, &P->d_cov, P->spec_elems() * sizeof(float)) != cudaSuccess ||
+        dmalloc(P, &P->d_covp, P->spec_elems() * sizeof(float)) != cudaSuccess)
       return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (Kalman state)"));
   }
   for (auto& sg : P->stages) {
-    if (cudaMallocPitch(&sg.in, &sg.in_pitch, (size_t)d->width * P->bytes, d->height) != cudaSuccess ||
-        cudaMallocPitch(&sg.out, &sg.out_pitch, (size_t)d->width * P->bytes, d->height) != cudaSuccess ||
+    if (dmalloc_pitch(P, &sg.in, &sg.in_pitch, (size_t)d->width * P->bytes, d->height) != cudaSuccess ||
+        dmalloc_pitch(P, &sg.out, &sg.out_pitch, (size_t)d->width * P->bytes, d->height) != cudaSuccess ||
         cudaMallocHost(&sg.h_flags, 2 * sizeof(int)) != cudaSuccess)
       return bail(fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (staging)"));
     if (cudaEventCreateWithFlags(&sg.in_free, cudaEventDisableTiming) != cudaSuccess ||
@@ -1765,7 +1801,7 @@ int fft3d_plane_set_psd(fft3d_plane* P, fft3d_psd* m, int pooled, float strength
       fft3d::psd::check_plane(m, P->device, P->g.bw, P->g.bh, P->g.ow, P->g.oh, P->ep.wintype);
   if (!why.empty()) return fail(FFT3D_E_UNSUPPORTED, "neo_fft3d: " + why);
   if (!P->d_psd) {
-    if (cudaMalloc(&P->d_psd, P->spec_elems() * sizeof(float)) != cudaSuccess) {
+    if (dmalloc(P, &P->d_psd, P->spec_elems() * sizeof(float)) != cudaSuccess) {
       cudaGetLastError();
       P->d_psd = nullptr;
       return fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory for the learned noise power");
@@ -1781,6 +1817,43 @@ int fft3d_plane_set_psd(fft3d_plane* P, fft3d_psd* m, int pooled, float strength
   P->psd_model = m;
   P->psd_pooled = pooled ? 1 : 0;
   P->psd_strength = strength;
+  return FFT3D_OK;
+}
+
+int fft3d_plane_device_bytes(fft3d_plane* P, uint64_t* out) {
+  if (!P || !out) return fail(FFT3D_E_PARAM, "neo_fft3d: null argument");
+  std::lock_guard<std::mutex> lk(P->mu);
+  *out = P->alloc_used;
+  return FFT3D_OK;
+}
+
+int fft3d_plane_synchronize(fft3d_plane* P) {
+  if (!P) return fail(FFT3D_E_PARAM, "neo_fft3d: null handle");
+  std::lock_guard<std::mutex> lk(P->mu);
+  CK(cudaSetDevice(P->device), "cudaSetDevice");
+  if (P->last_work) CK(cudaEventSynchronize(P->last_work), "synchronize");
+  for (auto* st : {P->s_up, P->stream, P->s_down}) CK(cudaStreamSynchronize(st), "synchronize");
+  int flags[2] = {0, 0};
+  CK(cudaMemcpy(&flags[0], P->d_err, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
+  if (P->psd_model) CK(cudaMemcpy(&flags[1], fft3d::psd::err_flag(P->psd_model), sizeof(int), cudaMemcpyDeviceToHost),
+                       "error flag");
+  for (int k = 0; k < 2; k++) {
+    if (!flags[k]) continue;
+    CK(cudaMemset(k == 0 ? P->d_err : fft3d::psd::err_flag(P->psd_model), 0, sizeof(int)), "error flag");
+    return fail(FFT3D_E_CUDA, (flags[k] & 2) ? "neo_fft3d: bulk copy completion wait timed out"
+                                             : "neo_fft3d: tensor-core MMA completion wait timed out");
+  }
+  return FFT3D_OK;
+}
+
+int fft3d_plane_debug_set_error_flag(fft3d_plane* P, int bits) {
+  if (!P) return fail(FFT3D_E_PARAM, "neo_fft3d: null handle");
+  std::lock_guard<std::mutex> lk(P->mu);
+  CK(cudaSetDevice(P->device), "cudaSetDevice");
+  // after the work already queued for the plane, like a kernel of the next call
+  if (P->last_work) CK(cudaEventSynchronize(P->last_work), "synchronize");
+  CK(cudaStreamSynchronize(P->stream), "synchronize");
+  CK(cudaMemcpy(P->d_err, &bits, sizeof(int), cudaMemcpyHostToDevice), "error flag");
   return FFT3D_OK;
 }
 

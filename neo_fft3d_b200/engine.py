@@ -20,7 +20,8 @@ _lib = None
 SYMBOLS = ("fft3d_params_default", "fft3d_plane_create", "fft3d_plane_filter", "fft3d_plane_filter_device",
            "fft3d_plane_cached", "fft3d_plane_spectrum", "fft3d_plane_geometry", "fft3d_plane_set_pattern_frame",
            "fft3d_plane_reset", "fft3d_plane_destroy", "fft3d_last_error", "fft3d_kernel_launches",
-           "fft3d_plane_set_timing", "fft3d_plane_timing")
+           "fft3d_plane_set_timing", "fft3d_plane_timing", "fft3d_plane_device_bytes", "fft3d_plane_synchronize",
+           "fft3d_plane_debug_set_error_flag")
 KERNELS = ("forward", "filter_inverse", "overlap_add", "fused", "filter_bins")
 
 
@@ -53,6 +54,9 @@ def lib():
         L.fft3d_plane_destroy.argtypes = [vp]
         L.fft3d_last_error.restype = ctypes.c_char_p
         L.fft3d_kernel_launches.restype = ctypes.c_uint64
+        L.fft3d_plane_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64)]
+        L.fft3d_plane_synchronize.argtypes = [vp]
+        L.fft3d_plane_debug_set_error_flag.argtypes = [vp, ci]
         L.fft3d_plane_set_timing.argtypes = [vp, ci]
         L.fft3d_plane_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
         L.fft3d_plane_set_psd.argtypes = [vp, vp, ci, ctypes.c_float]
@@ -170,6 +174,15 @@ class PlaneEngine:
 
     def reset(self):
         _check(lib().fft3d_plane_reset(self.h))
+
+    def device_bytes(self) -> int:
+        out = ctypes.c_uint64()
+        _check(lib().fft3d_plane_device_bytes(self.h, ctypes.byref(out)))
+        return int(out.value)
+
+    def synchronize(self):
+        """Wait for the plane's queued work; raises on a device-side wait that ran out."""
+        _check(lib().fft3d_plane_synchronize(self.h))
 
     def close(self):
         if getattr(self, "h", None):
