@@ -93,6 +93,15 @@ struct fft3d_plane {
   // to tdom_extra[k - 1]; frames in [keep_lo, keep_hi] stay in the ring while
   // the group is planned; all frames of a group use one CTA order.
   std::vector<float*> tdom_extra;
+  // filtered spectra of a frame group's frames (the two-pass group filter:
+  // k_filter_frames, then the sharpen/inverse pass on these), grown on first use
+  std::vector<float2*> filt_frames;
+  // how frame groups filter (NEO_FFT3D_GROUP_FILTER): 2 (default, =block):
+  // one launch per run of frames of one mode with one CTA per block, each
+  // window spectrum read once for the run; 1 (=split): a streaming filter
+  // launch for the run, then a sharpen/inverse launch; 0 (=fused): one
+  // filter/inverse launch per Wiener 3D run, frames interleaved by CTA
+  int group_split = 2;
   int occ = 0;
   int keep_lo = 1, keep_hi = 0;
   int fixed_reverse = -1;
@@ -354,6 +363,7 @@ void free_plane(fft3d_plane* P) {
   cudaFree(P->d_pshow);
   cudaFree(P->d_pshow_win);
   for (auto* t : P->tdom_extra) cudaFree(t);
+  for (auto* f : P->filt_frames) cudaFree(f);
   cudaFree(P->d_filt);
   cudaFree(P->d_tc);
   cudaFree(P->d_err);
@@ -974,6 +984,14 @@ int group_resources(fft3d_plane* P, int lo, int hi, int count) {
     }
     P->tdom_extra.push_back(t);
   }
+  while (P->group_split == 1 && (int)P->filt_frames.size() < count) {
+    float2* f = nullptr;
+    if (dmalloc(P, &f, P->spec_elems() * sizeof(float2)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(FFT3D_E_NOMEM, "neo_fft3d: out of device memory (filtered spectra of a frame group)");
+    }
+    P->filt_frames.push_back(f);
+  }
   return FFT3D_OK;
 }
 
@@ -1016,7 +1034,82 @@ int run_group(fft3d_plane* P, const fft3d::Deferred& d, cudaStream_t st) {
     g_launches++;
     i = e;
   }
-  for (size_t i = 0; i < d.inv.size();) {
+  for (size_t i = 0; P->group_split == 2 && i < d.inv.size();) {
+    // One launch per run of up to kGroupTile consecutive frames of one mode,
+    // one CTA per block: each window spectrum (and a Kalman state) is read
+    // once for the run and every filtered tile stays in shared memory.
+    const int mode = d.inv[i].mode;
+    size_t e = i + 1;
+    while (e < d.inv.size() && d.inv[e].mode == mode && (int)(e - i) < fft3d::kGroupTile) e++;
+    const int n = (int)(e - i);
+    fft3d::TemporalSet ts{};
+    ts.count = n;
+    std::vector<const float2*> seen;
+    for (size_t k = i; k < e; k++) {
+      for (int w = 0; w < 5; w++) {
+        const float2* sp = d.inv[k].a.in[w];
+        if (!sp) continue;
+        ts.spec[(k - i) + w] = sp;
+        if (std::find(seen.begin(), seen.end(), sp) == seen.end()) seen.push_back(sp);
+      }
+      ts.tdom[k - i] = d.inv[k].a.tdom;
+    }
+    const double state = mode == fft3d::MODE_KALMAN ? 2.0 * (double)P->spec_elems() * 16 : 0.0;
+    // reads: each window spectrum of the run once (+ Kalman state); writes: the time-domain blocks
+    TimeScope tsc(P, K_INVERSE, (double)seen.size() * S + state + n * T, st);
+    fft3d::InverseArgs ga = d.inv[i].a;
+    for (auto& p : ga.in) p = nullptr;
+    CK(fft3d::launch_filter_inverse_group(ga, ts, mode, st), "filter/inverse kernel (frame group)");
+    g_launches++;
+    i = e;
+  }
+  for (size_t i = 0; P->group_split == 1 && i < d.inv.size();) {
+    // Two passes per run of consecutive frames of one mode: the filter of all
+    // the run's frames (each window spectrum and the Kalman state read once),
+    // then the sharpen/dehalo pass and the inverse transform of each frame.
+    const int mode = d.inv[i].mode;
+    size_t e = i + 1;
+    while (e < d.inv.size() && d.inv[e].mode == mode && (int)(e - i) < fft3d::kMaxGroupFrames &&
+           (int)(e - i) < (int)P->filt_frames.size())
+      e++;
+    const int n = (int)(e - i);
+    fft3d::FrameSet fs{};
+    fs.count = n;
+    if (mode != fft3d::MODE_SHARPEN_ONLY) {
+      fft3d::FilterFrameSet ff{};
+      ff.count = n;
+      std::vector<const float2*> seen;
+      for (size_t k = i; k < e; k++) {
+        for (int w = 0; w < 5; w++) {
+          const float2* sp = d.inv[k].a.in[w];
+          if (!sp) continue;
+          ff.spec[(k - i) + w] = sp;
+          if (std::find(seen.begin(), seen.end(), sp) == seen.end()) seen.push_back(sp);
+        }
+        ff.out[k - i] = P->filt_frames[k - i];
+      }
+      const double state = mode == fft3d::MODE_KALMAN ? 2.0 * (double)P->spec_elems() * 16 : 0.0;
+      // reads: each window spectrum of the run once (+ Kalman state); writes: the filtered spectra
+      TimeScope ts(P, K_FILTER, (double)seen.size() * S + state + n * S, st);
+      CK(fft3d::launch_filter_frames(d.inv[i].a, ff, mode, st), "filter kernel (frame group)");
+      g_launches++;
+    }
+    for (size_t k = i; k < e; k++) {
+      fs.in[k - i][2] = mode == fft3d::MODE_SHARPEN_ONLY ? d.inv[k].a.in[2] : P->filt_frames[k - i];
+      fs.tdom[k - i] = d.inv[k].a.tdom;
+    }
+    {
+      // reads: the filtered spectra; writes: the time-domain blocks
+      TimeScope ts(P, K_INVERSE, n * (S + T), st);
+      fft3d::InverseArgs sa = d.inv[i].a;
+      for (auto& p : sa.in) p = nullptr;
+      CK(fft3d::launch_filter_inverse_frames(sa, fs, fft3d::MODE_SHARPEN_ONLY, st),
+         "sharpen/inverse kernel (frame group)");
+      g_launches++;
+    }
+    i = e;
+  }
+  for (size_t i = 0; !P->group_split && i < d.inv.size();) {
     const int mode = d.inv[i].mode;
     size_t e = i + 1;
     if (mode >= 2)
@@ -1421,6 +1514,9 @@ int fft3d_plane_create(const fft3d_params* p, const fft3d_plane_desc* d, int dev
     // filter/inverse kernel of the unfused and tc paths: register-pipelined (default) or bulk-staged
     const char* iv = std::getenv("NEO_FFT3D_INV");
     P->bulk = iv && std::string(iv) == "bulk";
+    const char* gf = std::getenv("NEO_FFT3D_GROUP_FILTER");
+    const std::string gv = gf ? gf : "block";
+    P->group_split = gv == "fused" ? 0 : (gv == "split" ? 1 : 2);
   }
   fft3d_params& ep = P->ep;
   if (d->bits < 8 || (d->bits > 16 && d->bits != 32)) { delete P; return fail(FFT3D_E_PARAM, "neo_fft3d: unsupported bit depth"); }

@@ -294,6 +294,28 @@ cudaError_t launch_filter_bins(const InverseArgs& a, float2* F, int mode, cudaSt
   return cudaGetLastError();
 }
 
+cudaError_t launch_filter_inverse_group(const InverseArgs& a, const TemporalSet& ts, int mode, cudaStream_t s) {
+  const SizeEntry* e = find_size(a.g.bw, a.g.bh);
+  return e ? e->inv_group(a, ts, mode, s) : cudaErrorInvalidValue;
+}
+
+cudaError_t launch_filter_frames(const InverseArgs& a, const FilterFrameSet& fs, int mode, cudaStream_t s) {
+  if (fs.count < 1 || fs.count > kMaxGroupFrames) return cudaErrorInvalidValue;
+  const int bins = a.g.bh * a.g.nh;
+  const size_t pairs = (size_t)a.g.nblocks * bins / 2;
+  const int grid = (int)((pairs + 255) / 256);
+  switch (mode) {
+    case MODE_KALMAN: k_filter_frames<MODE_KALMAN><<<grid, 256, 0, s>>>(a, fs, bins); break;
+    case 1: k_filter_frames<1><<<grid, 256, 0, s>>>(a, fs, bins); break;
+    case 2: k_filter_frames<2><<<grid, 256, 0, s>>>(a, fs, bins); break;
+    case 3: k_filter_frames<3><<<grid, 256, 0, s>>>(a, fs, bins); break;
+    case 4: k_filter_frames<4><<<grid, 256, 0, s>>>(a, fs, bins); break;
+    case 5: k_filter_frames<5><<<grid, 256, 0, s>>>(a, fs, bins); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_fused(const FusedArgs& a, int mode, int bytes, cudaStream_t s) {
   const SizeEntry* e = find_size(a.v.g.bw, a.v.g.bh);
   return e ? e->fused(a, mode, bytes, s) : cudaErrorInvalidValue;

@@ -106,6 +106,29 @@ struct FrameSet {
   int count;
 };
 
+// The filter of a run of consecutive output frames n0 .. n0 + count - 1 of one
+// plane with one mode in one launch (k_filter_frames): spec[s] is the
+// spectrum of frame n0 - 2 + s (s < count + 4; null where no window of the
+// run reaches), out[j] receives frame n0 + j's filtered spectrum (blocks x
+// bh x nh complex, unpadded like the ring).
+struct FilterFrameSet {
+  const float2* spec[kMaxGroupFrames + 4];
+  float2* out[kMaxGroupFrames];
+  int count;
+};
+
+// A run of consecutive output frames n0 .. n0 + count - 1 (count <=
+// kGroupTile) of one plane with one mode, filtered and inverse-transformed
+// by one launch with one CTA per block (k_filter_inverse_group): spec[s] is
+// the spectrum of frame n0 - 2 + s (null where no window of the run reaches),
+// tdom[j] receives frame n0 + j's time-domain blocks.
+constexpr int kGroupTile = 8;
+struct TemporalSet {
+  const float2* spec[kGroupTile + 4];
+  float* tdom[kGroupTile];
+  int count;
+};
+
 // The new frames of a frame group, transformed by one launch: frame j's
 // samples (src/stride as in ForwardArgs) and ring slot. ctas: CTAs per frame
 // (set by the launcher).
@@ -172,6 +195,9 @@ cudaError_t launch_filter_inverse(const InverseArgs& a, int mode, cudaStream_t s
 // Frame group: fs.count consecutive output frames of one plane (Wiener 3D,
 // mode 2..5) in one launch; a holds everything they share.
 cudaError_t launch_filter_inverse_frames(const InverseArgs& a, const FrameSet& fs, int mode, cudaStream_t s);
+// A run of frames of one plane in one launch, each block's spectra read once
+// for the whole run (modes -1..5; Kalman runs in frame order).
+cudaError_t launch_filter_inverse_group(const InverseArgs& a, const TemporalSet& ts, int mode, cudaStream_t s);
 // Forward transforms of fs.count frames of one plane in one launch; a holds
 // what they share (geometry, windows, sample offset).
 cudaError_t launch_forward_frames(const ForwardArgs& a, const FwdFrameSet& fs, int bytes_per_sample, cudaStream_t s);
@@ -194,6 +220,11 @@ int batch_occupancy(int bw, int bh, int which, int mode_or_bytes);  // which: 0 
 // Streaming filter of all bins (Wiener 2D/3D, Kalman) into F; the sharpen pass
 // and the inverse follow with launch_filter_inverse(MODE_SHARPEN_ONLY) on F.
 cudaError_t launch_filter_bins(const InverseArgs& a, float2* F, int mode, cudaStream_t s);
+// Filter of a run of frames of one plane (Wiener 2D/3D or Kalman; the
+// sharpen pass and the inverse follow with launch_filter_inverse_frames in
+// MODE_SHARPEN_ONLY on fs.out). Kalman runs walk the frames in order, with
+// the state in registers from the run's first frame to its last.
+cudaError_t launch_filter_frames(const InverseArgs& a, const FilterFrameSet& fs, int mode, cudaStream_t s);
 // cudaErrorNotSupported when no fused kernel exists for the sample type (float)
 cudaError_t launch_fused(const FusedArgs& a, int mode, int bytes_per_sample, cudaStream_t s);
 bool block_size_supported(int bw, int bh);

@@ -71,9 +71,11 @@ __device__ __forceinline__ void load_row(const T* p, float (&r)[BW]) {
         constexpr int PER = 16 / (int)sizeof(T);
 #pragma unroll
         for (int j = 0; j < PER; j++) {
-          float f;
-          if constexpr (sizeof(T) == 1) f = (float)((w[j >> 2] >> (8 * (j & 3))) & 0xffu);
-          else if constexpr (sizeof(T) == 2) f = (float)((w[j >> 1] >> (16 * (j & 1))) & 0xffffu);
+          float f;  // 8/16-bit: exact through the 2^23 mantissa trick (decode_row)
+          if constexpr (sizeof(T) == 1)
+            f = __uint_as_float(__byte_perm(w[j >> 2], 0x4B000000u, 0x7540u | (uint32_t)(j & 3))) - 8388608.0f;
+          else if constexpr (sizeof(T) == 2)
+            f = __uint_as_float(__byte_perm(w[j >> 1], 0x4B000000u, (j & 1) ? 0x7432u : 0x7410u)) - 8388608.0f;
           else f = __uint_as_float(w[j]);
           r[v * PER + j] = f;
         }
@@ -124,18 +126,25 @@ __host__ __device__ constexpr int raw_vectors() {
   return (sizeof(T) <= 2 && (BW * (int)sizeof(T)) % 16 == 0) ? BW * (int)sizeof(T) / 16 : 0;
 }
 
+// Samples minus `base` as floats, decoded from raw 16-byte vectors. Each
+// 8/16-bit sample is placed by one byte permute into the low mantissa bits of
+// 2^23 (0x4B000000 + v is exactly the float 2^23 + v for v < 2^23), and one
+// FADD of -(2^23 + base) leaves v - base exactly: an ALU permute and an FMA-pipe
+// add per sample instead of shift/mask and an int-to-float conversion on the
+// narrower conversion pipe.
 template <int BW, typename T>
-__device__ __forceinline__ void decode_row(const uint4* raw, float (&r)[BW]) {
+__device__ __forceinline__ void decode_row(const uint4* raw, float base, float (&r)[BW]) {
   constexpr int PER = 16 / (int)sizeof(T);
+  const float off = 8388608.0f + base;  // exact: base <= 2^15
 #pragma unroll
   for (int v = 0; v < raw_vectors<BW, T>(); v++) {
     const uint32_t w[4] = {raw[v].x, raw[v].y, raw[v].z, raw[v].w};
 #pragma unroll
     for (int j = 0; j < PER; j++) {
-      float f;
-      if constexpr (sizeof(T) == 1) f = (float)((w[j >> 2] >> (8 * (j & 3))) & 0xffu);
-      else f = (float)((w[j >> 1] >> (16 * (j & 1))) & 0xffffu);
-      r[v * PER + j] = f;
+      uint32_t m;
+      if constexpr (sizeof(T) == 1) m = __byte_perm(w[j >> 2], 0x4B000000u, 0x7540u | (uint32_t)(j & 3));
+      else m = __byte_perm(w[j >> 1], 0x4B000000u, (j & 1) ? 0x7432u : 0x7410u);
+      r[v * PER + j] = __uint_as_float(m) - off;
     }
   }
 }
@@ -152,19 +161,23 @@ __device__ __forceinline__ void fwd_row(const ForwardArgs& a, const Win& win, in
   const T* srow = fwd_row_src<T>(a, win, blk, y, &x0);
   float r[BW];
   if constexpr (raw_vectors<BW, T>() > 0) {
-    if (raw) decode_row<BW, T>(raw, r);
+    if (raw) decode_row<BW, T>(raw, a.base, r);  // already minus base
   }
   if (raw_vectors<BW, T>() > 0 && raw) {
-  } else if (x0 >= 0 && x0 + BW <= g.W) {
-    load_row<T, BW>(srow + x0, r);
   } else {
+    if (x0 >= 0 && x0 + BW <= g.W) {
+      load_row<T, BW>(srow + x0, r);
+    } else {
 #pragma unroll
-    for (int x = 0; x < BW; x++) r[x] = load_sample<T>(srow + reflect101(x0 + x, g.W));
+      for (int x = 0; x < BW; x++) r[x] = load_sample<T>(srow + reflect101(x0 + x, g.W));
+    }
+#pragma unroll
+    for (int x = 0; x < BW; x++) r[x] = r[x] - a.base;
   }
   const float wy = __ldg(a.wan_y + y);
   // the x window from the launch parameters (ARGS_WX) or from the table
 #pragma unroll
-  for (int x = 0; x < BW; x++) r[x] = (r[x] - a.base) * (ARGS_WX ? a.wx[x] : __ldg(a.wan_x + x)) * wy;
+  for (int x = 0; x < BW; x++) r[x] = r[x] * (ARGS_WX ? a.wx[x] : __ldg(a.wan_x + x)) * wy;
   float2 c[NH];
   rfft<BW>(r, c);
   float2* row = Sb + y * NH;
@@ -386,21 +399,28 @@ __device__ __forceinline__ BinTab bin_tab(const InverseArgs& a, int bin) {
   return t;
 }
 
+// |c|^2 + 1e-15 of a bin (the reference's psd, src/code_impl/Apply.cpp:27-31)
+__device__ __forceinline__ float bin_psd(float re, float im) { return fmaf(re, re, fmaf(im, im, 1.0e-15f)); }
+
 __device__ __forceinline__ float sharpen_fact(const InverseArgs& a, float psd, float wsh) {
-  // src/code_impl/Apply.cpp:129-131
-  return 1.f + a.c.sharpen * wsh * sqrtf(__fdividef(psd * a.c.smax2n, (psd + a.c.smin2n) * (psd + a.c.smax2n)));
+  // src/code_impl/Apply.cpp:129-131: 1 + sharpen * wsh * sqrt(N / D) with
+  // N = psd * smax2n, D = (psd + smin2n)(psd + smax2n), evaluated as
+  // N * rsqrt(N * D) (N = 0 when smax = 0: the clamp keeps 0 * rsqrt finite)
+  const float n = psd * a.c.smax2n;
+  const float d = (psd + a.c.smin2n) * (psd + a.c.smax2n);
+  return fmaf(a.c.sharpen * wsh, n * rsqrtf(fmaxf(n * d, 1e-30f)), 1.f);
 }
 __device__ __forceinline__ float dehalo_fact(const InverseArgs& a, float psd, float wdh) {
   // src/code_impl/Apply.cpp:132
   return __fdividef(psd + a.c.ht2n, (psd + a.c.ht2n) + a.c.dehalo * wdh * psd);
 }
 
-// limited Wiener factor applied to one temporal component, code_impl_C.h:34-40
-// (divisions use the fast reciprocal: <= 2 ulp, far inside the +-1 LSB output bar)
+// limited Wiener factor applied to one temporal component, code_impl_C.h:34-40:
+// max((psd - noise) / psd, lowlimit) as max(1 - noise / psd, lowlimit) with
+// the fast reciprocal (<= 2 ulp, far inside the +-1 LSB output bar)
 __device__ __forceinline__ void wiener(float& re, float& im, float noise, float lowlimit) {
-  const float psd = re * re + im * im + 1.0e-15f;
-  const float q = __fdividef(psd - noise, psd);
-  const float f = q > lowlimit ? q : lowlimit;
+  const float q = fmaf(-noise, __fdividef(1.f, bin_psd(re, im)), 1.f);
+  const float f = fmaxf(q, lowlimit);
   re *= f;
   im *= f;
 }
@@ -408,6 +428,27 @@ __device__ __forceinline__ void wiener(float& re, float& im, float noise, float 
 // Learned noise power of bin `bin` of the block at spectrum offset `off`.
 __device__ __forceinline__ float learned_noise(const InverseArgs& a, size_t off, int bin) {
   return a.psd_scale * __ldg(a.psd + (a.psd_per_block ? off : 0) + bin);
+}
+
+// One Kalman step of one bin, src/code_impl/Kalman.cpp:27-64: the motion test
+// per component (OR), then either a reset to the current value or the gain
+// update; last/cv/cp are the bin's state (filtered value, covariance, process
+// covariance), updated in place. `sigma` is the bin's noise power.
+__device__ __forceinline__ void kalman_step(const InverseArgs& a, float2 cur, float sigma, float2& last, float& cv,
+                                            float& cp) {
+  const float dr = cur.x - last.x, di = cur.y - last.y;
+  if (dr * dr > sigma * a.c.kratio2 || di * di > sigma * a.c.kratio2) {
+    cv = sigma;
+    cp = sigma;
+    last = cur;
+  } else {
+    const float sum = cv + cp;
+    const float gain = __fdividef(sum, sum + sigma);
+    cp = gain * gain * sigma;
+    cv = (1.f - gain) * sum;
+    last.x = gain * cur.x + (1.f - gain) * last.x;
+    last.y = gain * cur.y + (1.f - gain) * last.y;
+  }
 }
 
 // Filtered value of one bin from its values w[0..4] in frames n-2..n+2 (only
@@ -435,19 +476,7 @@ __device__ __forceinline__ float2 filter_vals(const InverseArgs& a, const float2
       sigma = __ldg(a.t.pattern2d + bin);
       if (sigma < 1e-15f) sigma = 1e-15f;
     }
-    const float dr = cur.x - last.x, di = cur.y - last.y;
-    if (dr * dr > sigma * a.c.kratio2 || di * di > sigma * a.c.kratio2) {
-      cv = sigma;
-      cp = sigma;
-      last = cur;
-    } else {
-      const float sum = cv + cp;
-      const float gain = __fdividef(sum, sum + sigma);
-      cp = gain * gain * sigma;
-      cv = (1.f - gain) * sum;
-      last.x = gain * cur.x + (1.f - gain) * last.x;
-      last.y = gain * cur.y + (1.f - gain) * last.y;
-    }
+    kalman_step(a, cur, sigma, last, cv, cp);
     if (commit) {
       a.kal_last[off + bin] = last;
       a.kal_covar[off + bin] = cv;
@@ -459,10 +488,9 @@ __device__ __forceinline__ float2 filter_vals(const InverseArgs& a, const float2
     float2 gc = make_float2(0.f, 0.f);
     if (a.c.degrid != 0.f) gc = make_float2(gf * tb.grid.x, gf * tb.grid.y);
     const float cr = cur.x - gc.x, ci = cur.y - gc.y;
-    const float psd = cr * cr + ci * ci + 1e-15f;
+    const float psd = bin_psd(cr, ci);
     const float noise = a.psd ? learned_noise(a, off, bin) : a.c.pattern ? __ldg(a.t.pattern2d + bin) : a.c.sigma2n;
-    const float q = __fdividef(psd - noise, psd);
-    float f = q > a.c.lowlimit ? q : a.c.lowlimit;
+    float f = fmaxf(fmaf(-noise, __fdividef(1.f, psd), 1.f), a.c.lowlimit);
     if (a.c.fuse_sharpen) {
       if (a.c.use_sharpen && a.c.use_dehalo) f *= sharpen_fact(a, psd, tb.wsh) * dehalo_fact(a, psd, tb.wdh);
       else if (a.c.use_sharpen) f *= sharpen_fact(a, psd, tb.wsh);
@@ -471,11 +499,13 @@ __device__ __forceinline__ float2 filter_vals(const InverseArgs& a, const float2
     return make_float2(cr * f + gc.x, ci * f + gc.y);
   } else {
     // Wiener 3D over MODE frames, src/code_impl/Apply.cpp:67-235
-    constexpr float kb = (float)MODE;
+    // gc * bt (src/code_impl/Apply.cpp:78-93); gf * MODE is the same for every
+    // bin of the block and leaves the bin loop
+    const float gk = gf * (float)MODE;
     float g0 = 0.f, g1 = 0.f;
     if (a.c.degrid != 0.f) {
-      g0 = gf * tb.grid.x * kb;
-      g1 = gf * tb.grid.y * kb;
+      g0 = gk * tb.grid.x;
+      g1 = gk * tb.grid.y;
     }
     const float noise = a.psd ? learned_noise(a, off, bin) : a.c.pattern ? __ldg(a.t.pattern3d + bin) : a.c.sigma2n;
     const float ll = a.c.lowlimit;
@@ -562,7 +592,7 @@ __device__ __forceinline__ float2 sharpen_bin(const InverseArgs& a, float2 v, co
   float2 gc = make_float2(0.f, 0.f);
   if (a.c.degrid != 0.f) gc = make_float2(gf * tb.grid.x, gf * tb.grid.y);
   const float cr = v.x - gc.x, ci = v.y - gc.y;
-  const float psd = cr * cr + ci * ci + 1.0e-15f;
+  const float psd = bin_psd(cr, ci);
   float f;
   if (a.c.use_sharpen && a.c.use_dehalo) f = sharpen_fact(a, psd, tb.wsh) * dehalo_fact(a, psd, tb.wdh);
   else if (a.c.use_sharpen) f = sharpen_fact(a, psd, tb.wsh);
@@ -571,6 +601,14 @@ __device__ __forceinline__ float2 sharpen_bin(const InverseArgs& a, float2 v, co
 }
 
 // ---------------------------------------------------------------- filter (streaming)
+
+// Two neighbouring bins of a window spectrum, read once per thread: not kept
+// in L1 (the per-bin tables stay there).
+__device__ __forceinline__ float4 ld_stream4(const float2* p) {
+  float4 v;
+  asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+  return v;
+}
 
 // Filter of every bin of every block as a flat stream: each thread takes two
 // neighbouring bins (one 16-byte load per window frame, one 16-byte store of
@@ -601,6 +639,74 @@ __global__ void __launch_bounds__(256) k_filter_bins(InverseArgs a, float2* F, i
     const float2 v0 = filter_vals<MODE>(a, w0, off, bin, gf, bin_tab<MODE>(a, bin), true);
     const float2 v1 = filter_vals<MODE>(a, w1, off, bin + 1, gf, bin_tab<MODE>(a, bin + 1), true);
     reinterpret_cast<float4*>(F)[q] = make_float4(v0.x, v0.y, v1.x, v1.y);
+  }
+}
+
+// Filter of a run of consecutive output frames of one plane (a frame group)
+// in one launch: each thread takes two neighbouring bins of one block and
+// walks the run's frames in order with the bins' temporal window in
+// registers, so that every window spectrum is loaded once per run (not once
+// per output frame), and a Kalman state once per run. fs.spec[s] is frame
+// n0 - 2 + s; frame n0 + j's window is fs.spec[j + LO .. j + HI] and its
+// filtered bins go to fs.out[j]. The sharpen/dehalo pass and the inverse
+// transform follow per frame (k_filter_inverse_frames<MODE_SHARPEN_ONLY> on
+// fs.out[j]). Few registers and no shared memory: the SMs hold enough warps
+// to cover the load latency by themselves.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_filter_frames(InverseArgs a, const __grid_constant__ FilterFrameSet fs,
+                                                     int bins_per_block) {
+  constexpr int LO = win_lo<MODE>(), HI = win_hi<MODE>(), NW = HI - LO + 1;
+  const size_t pairs = (size_t)a.g.nblocks * bins_per_block / 2;
+  const float gs0 = __ldg(&a.t.grid[0].x);
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < pairs; q += (size_t)gridDim.x * blockDim.x) {
+    const size_t e = 2 * q;
+    const int bin = (int)(e % bins_per_block);
+    const size_t off = e - bin;
+    const BinTab tb0 = bin_tab<MODE>(a, bin), tb1 = bin_tab<MODE>(a, bin + 1);
+    if constexpr (MODE == MODE_KALMAN) {
+      // the state of both bins stays in registers across the run's frames
+      float4 lv;
+      float2 cv, cp;
+      asm("ld.global.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+          : "=f"(lv.x), "=f"(lv.y), "=f"(lv.z), "=f"(lv.w) : "l"(a.kal_last + e));
+      asm("ld.global.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(cv.x), "=f"(cv.y) : "l"(a.kal_covar + e));
+      asm("ld.global.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(cp.x), "=f"(cp.y) : "l"(a.kal_covarp + e));
+      float2 l0 = make_float2(lv.x, lv.y), l1 = make_float2(lv.z, lv.w);
+      float s0 = a.c.sigma2n_2d, s1 = a.c.sigma2n_2d;
+      if (a.c.pattern) {
+        s0 = fmaxf(__ldg(a.t.pattern2d + bin), 1e-15f);
+        s1 = fmaxf(__ldg(a.t.pattern2d + bin + 1), 1e-15f);
+      }
+      for (int j = 0; j < fs.count; j++) {
+        const float4 c = ld_stream4(fs.spec[j + 2] + e);
+        kalman_step(a, make_float2(c.x, c.y), s0, l0, cv.x, cp.x);
+        kalman_step(a, make_float2(c.z, c.w), s1, l1, cv.y, cp.y);
+        reinterpret_cast<float4*>(fs.out[j])[q] = make_float4(l0.x, l0.y, l1.x, l1.y);
+      }
+      reinterpret_cast<float4*>(a.kal_last)[q] = make_float4(l0.x, l0.y, l1.x, l1.y);
+      reinterpret_cast<float2*>(a.kal_covar)[q] = cv;
+      reinterpret_cast<float2*>(a.kal_covarp)[q] = cp;
+    } else {
+      float4 wv[NW];
+#pragma unroll
+      for (int k = 0; k < NW - 1; k++) wv[k] = ld_stream4(fs.spec[LO + k] + e);
+      for (int j = 0; j < fs.count; j++) {
+        wv[NW - 1] = ld_stream4(fs.spec[j + HI] + e);
+        const float gf = (MODE >= 1) ? a.c.degrid * __ldg(&fs.spec[j + 2][off].x) / gs0 : 0.f;
+        float2 w0[5], w1[5];
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+          const bool in = k >= LO && k <= HI;
+          w0[k] = in ? make_float2(wv[k - LO].x, wv[k - LO].y) : make_float2(0.f, 0.f);
+          w1[k] = in ? make_float2(wv[k - LO].z, wv[k - LO].w) : make_float2(0.f, 0.f);
+        }
+        const float2 v0 = filter_vals<MODE>(a, w0, off, bin, gf, tb0, false);
+        const float2 v1 = filter_vals<MODE>(a, w1, off, bin + 1, gf, tb1, false);
+        reinterpret_cast<float4*>(fs.out[j])[q] = make_float4(v0.x, v0.y, v1.x, v1.y);
+#pragma unroll
+        for (int k = 0; k < NW - 1; k++) wv[k] = wv[k + 1];
+      }
+    }
   }
 }
 
@@ -793,6 +899,219 @@ __global__ void __launch_bounds__(kWarps * 32) k_filter_inverse_batch(const Inve
     for (int w = threadIdx.x; w < (int)(sizeof(InverseArgs) / 4); w += blockDim.x) dst[w] = src[w];
     __syncthreads();
     filter_inverse_cta<BW, BH, MODE>(sa, it.y);
+  }
+}
+
+// ---------------------------------------------------------------- frame groups, one CTA per block
+
+// Dynamic shared memory of k_filter_inverse_group: two grid fractions per
+// frame (64 bytes), then `count` spectrum tiles.
+template <int BW, int BH>
+__host__ __device__ constexpr int group_smem_bytes(int count) {
+  return 2 * kGroupTile * 4 + count * BH * (BW / 2 + 1) * 8;
+}
+
+// A run of count <= kGroupTile consecutive output frames of one plane with
+// one mode; CTA = one block. Each stage is spread over the whole CTA, with a
+// barrier between stages:
+//  0. the grid fraction of each frame's block (its DC);
+//  1. filter: each thread takes two neighbouring bins and walks the run's
+//     frames in order, its window of MODE frames in registers (a circular
+//     buffer; the next frame's bins loaded one frame ahead), so that each of
+//     the block's count + MODE - 1 window spectra is read once for the run
+//     (and a Kalman state once); the filtered bins of frame j go to tile j in
+//     shared memory, and the thread holding the DC publishes each tile's
+//     filtered DC;
+//     (pairs beyond the last whole round of the CTA's threads are spread
+//     over all threads as single (pair, frame) items, so that no warp walks
+//     a third round alone);
+//  2. the separate sharpen/dehalo pass (src/code_impl/Sharpen.cpp:13-63), its
+//     grid fraction from each tile's filtered DC, the pair's tables loaded
+//     once for all frames;
+//  3. the inverse column DFTs of every tile (DC and Nyquist columns as one
+//     complex transform), 4. the c2r rows, 5. coalesced stores of the
+//     time-domain blocks.
+// Every bin and every transform uses the arithmetic of k_filter_inverse
+// (filter_vals, kalman_step, sharpen_bin, inv_col, inv_row_inplace), so the
+// output equals one frame per launch.
+template <int MODE>
+__device__ __forceinline__ void group_filter_pair(const InverseArgs& a, const TemporalSet& ts, size_t off, int bin,
+                                                  int count, const float* gfs, float* gsh, float gs0, float2* tile,
+                                                  int tile_stride) {
+  constexpr int LO = win_lo<MODE>(), HI = win_hi<MODE>(), NW = HI - LO + 1;
+  auto out = [&](int j, float2 v0, float2 v1) {
+    *reinterpret_cast<float4*>(tile + j * tile_stride) = make_float4(v0.x, v0.y, v1.x, v1.y);
+    if (bin == 0) gsh[j] = a.c.degrid * v0.x / gs0;  // the sharpen pass's grid fraction: the filtered DC
+  };
+  if constexpr (MODE == MODE_KALMAN) {
+    float4 lv;
+    float2 cv, cp;
+    asm("ld.global.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+        : "=f"(lv.x), "=f"(lv.y), "=f"(lv.z), "=f"(lv.w) : "l"(a.kal_last + off + bin));
+    asm("ld.global.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(cv.x), "=f"(cv.y) : "l"(a.kal_covar + off + bin));
+    asm("ld.global.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(cp.x), "=f"(cp.y) : "l"(a.kal_covarp + off + bin));
+    float2 l0 = make_float2(lv.x, lv.y), l1 = make_float2(lv.z, lv.w);
+    float s0 = a.c.sigma2n_2d, s1 = a.c.sigma2n_2d;
+    if (a.c.pattern) {
+      s0 = fmaxf(__ldg(a.t.pattern2d + bin), 1e-15f);
+      s1 = fmaxf(__ldg(a.t.pattern2d + bin + 1), 1e-15f);
+    }
+    float4 nxt = ld_stream4(ts.spec[2] + off + bin);
+    for (int j = 0; j < count; j++) {
+      const float4 c = nxt;
+      if (j + 1 < count) nxt = ld_stream4(ts.spec[j + 3] + off + bin);
+      kalman_step(a, make_float2(c.x, c.y), s0, l0, cv.x, cp.x);
+      kalman_step(a, make_float2(c.z, c.w), s1, l1, cv.y, cp.y);
+      out(j, l0, l1);
+    }
+    *reinterpret_cast<float4*>(a.kal_last + off + bin) = make_float4(l0.x, l0.y, l1.x, l1.y);
+    *reinterpret_cast<float2*>(a.kal_covar + off + bin) = cv;
+    *reinterpret_cast<float2*>(a.kal_covarp + off + bin) = cp;
+  } else if constexpr (MODE == MODE_SHARPEN_ONLY) {
+    for (int j = 0; j < count; j++) {
+      const float4 c = ld_stream4(ts.spec[j + 2] + off + bin);
+      out(j, make_float2(c.x, c.y), make_float2(c.z, c.w));
+    }
+  } else {
+    const BinTab tb0 = bin_tab<MODE>(a, bin), tb1 = bin_tab<MODE>(a, bin + 1);
+    // spectrum s (frame n0 - 2 + s) lives in r[s % NW]; frame j reads
+    // s = j + LO .. j + HI; with j = j0 + u and j0 a multiple of NW every
+    // index below is a compile-time constant
+    float4 r[NW];
+#pragma unroll
+    for (int k = 0; k < NW - 1; k++) r[(LO + k) % NW] = ld_stream4(ts.spec[LO + k] + off + bin);
+    float4 nxt = ld_stream4(ts.spec[HI] + off + bin);
+    for (int j0 = 0; j0 < count; j0 += NW) {
+#pragma unroll
+      for (int u = 0; u < NW; u++) {
+        const int j = j0 + u;
+        if (j < count) {
+          r[(u + HI) % NW] = nxt;
+          if (j + 1 < count) nxt = ld_stream4(ts.spec[j + 1 + HI] + off + bin);
+          float2 w0[5], w1[5];
+#pragma unroll
+          for (int k = 0; k < 5; k++) {
+            const bool in = k >= LO && k <= HI;
+            const float4 v = r[(u + (in ? k : LO)) % NW];
+            w0[k] = in ? make_float2(v.x, v.y) : make_float2(0.f, 0.f);
+            w1[k] = in ? make_float2(v.z, v.w) : make_float2(0.f, 0.f);
+          }
+          const float gf = gfs[j];
+          out(j, filter_vals<MODE>(a, w0, off, bin, gf, tb0, false), filter_vals<MODE>(a, w1, off, bin + 1, gf, tb1, false));
+        }
+      }
+    }
+  }
+}
+
+// One frame of one bin pair (the tail of the filter stage, spread over all
+// threads): the pair's window for frame j loaded directly. Wiener modes.
+template <int MODE>
+__device__ __forceinline__ void group_filter_one(const InverseArgs& a, const TemporalSet& ts, size_t off, int bin, int j,
+                                                 const float* gfs, float* gsh, float gs0, float2* tile) {
+  constexpr int LO = win_lo<MODE>(), HI = win_hi<MODE>();
+  float4 r[5];
+#pragma unroll
+  for (int k = LO; k <= HI; k++) r[k] = ld_stream4(ts.spec[j + k] + off + bin);
+  float2 w0[5], w1[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    const bool in = k >= LO && k <= HI;
+    w0[k] = in ? make_float2(r[k].x, r[k].y) : make_float2(0.f, 0.f);
+    w1[k] = in ? make_float2(r[k].z, r[k].w) : make_float2(0.f, 0.f);
+  }
+  float2 v0, v1;
+  if constexpr (MODE == MODE_SHARPEN_ONLY) {
+    v0 = w0[2];
+    v1 = w1[2];
+  } else {
+    v0 = filter_vals<MODE>(a, w0, off, bin, gfs[j], bin_tab<MODE>(a, bin), false);
+    v1 = filter_vals<MODE>(a, w1, off, bin + 1, gfs[j], bin_tab<MODE>(a, bin + 1), false);
+  }
+  *reinterpret_cast<float4*>(tile) = make_float4(v0.x, v0.y, v1.x, v1.y);
+  if (bin == 0) gsh[j] = a.c.degrid * v0.x / gs0;
+}
+
+template <int BW, int BH, int MODE>
+__global__ void __launch_bounds__(kWarps * 32, 5) k_filter_inverse_group(InverseArgs a,
+                                                                     const __grid_constant__ TemporalSet ts) {
+  constexpr int NH = BW / 2 + 1, HC = BW / 2, BINS = BH * NH, PAIRS = BINS / 2, NT = kWarps * 32;
+  static_assert(BINS % 2 == 0, "bin pairs");
+  extern __shared__ float2 smem2[];
+  float* gfs = reinterpret_cast<float*>(smem2);  // grid fraction of each frame's block
+  float* gsh = gfs + kGroupTile;                 // ... and of its filtered block (sharpen pass)
+  float2* S = smem2 + kGroupTile;                // [count][BINS] tiles, 16-byte aligned
+  const int count = ts.count;
+  const size_t off = (size_t)blockIdx.x * BINS;
+  const float gs0 = __ldg(&a.t.grid[0].x);
+  const int t = threadIdx.x;
+  // 0. grid fraction of each frame's block (its DC)
+  if (MODE >= 1 && t < count) gfs[t] = a.c.degrid * __ldg(&ts.spec[t + 2][off].x) / gs0;
+  __syncthreads();
+  // 1. filter: whole rounds of bin pairs over all frames; the remaining pairs
+  //    (a partial round) as (pair, frame) items spread over every thread,
+  //    except for Kalman, whose frames follow one another
+  constexpr int FULL = (PAIRS / NT) * NT;
+  for (int p = t; p < FULL; p += NT)
+    group_filter_pair<MODE>(a, ts, off, 2 * p, count, gfs, gsh, gs0, S + 2 * p, BINS);
+  if constexpr (MODE == MODE_KALMAN) {
+    for (int p = FULL + t; p < PAIRS; p += NT)
+      group_filter_pair<MODE>(a, ts, off, 2 * p, count, gfs, gsh, gs0, S + 2 * p, BINS);
+  } else {
+    for (int i = t; i < (PAIRS - FULL) * count; i += NT) {
+      const int q = i / count, j = i - q * count, p = FULL + q;
+      group_filter_one<MODE>(a, ts, off, 2 * p, j, gfs, gsh, gs0, S + j * BINS + 2 * p);
+    }
+  }
+  __syncthreads();
+  // 2. the separate sharpen/dehalo pass (src/code_impl/Sharpen.cpp:13-63),
+  //    its grid fraction from each tile's filtered DC (published by the
+  //    filter stage); per bin pair, the pair's tables loaded once for all frames
+  if (a.c.do_sharpen) {
+    for (int p = t; p < PAIRS; p += NT) {
+      const int bin = 2 * p;
+      BinTab tb0{make_float2(0.f, 0.f), 0.f, 0.f}, tb1 = tb0;
+      if (a.c.degrid != 0.f) {
+        const float4 g = __ldg(reinterpret_cast<const float4*>(a.t.grid + bin));
+        tb0.grid = make_float2(g.x, g.y);
+        tb1.grid = make_float2(g.z, g.w);
+      }
+      if (a.c.use_sharpen) {
+        tb0.wsh = __ldg(a.t.wsharpen + bin);
+        tb1.wsh = __ldg(a.t.wsharpen + bin + 1);
+      }
+      if (a.c.use_dehalo) {
+        tb0.wdh = __ldg(a.t.wdehalo + bin);
+        tb1.wdh = __ldg(a.t.wdehalo + bin + 1);
+      }
+      for (int j = 0; j < count; j++) {
+        float4* q = reinterpret_cast<float4*>(S + j * BINS + bin);
+        const float4 v = *q;
+        const float2 v0 = sharpen_bin(a, make_float2(v.x, v.y), tb0, gsh[j]);
+        const float2 v1 = sharpen_bin(a, make_float2(v.z, v.w), tb1, gsh[j]);
+        *q = make_float4(v0.x, v0.y, v1.x, v1.y);
+      }
+    }
+    __syncthreads();
+  }
+  // 3. inverse column DFTs
+  for (int i = t; i < count * HC; i += NT) {
+    const int j = i / HC;
+    inv_col<BW, BH>(S + j * BINS, i - j * HC);
+  }
+  __syncthreads();
+  // 4. c2r rows, in place
+  for (int i = t; i < count * BH; i += NT) {
+    const int j = i / BH;
+    inv_row_inplace<BW, BH>(S + j * BINS, i - j * BH);
+  }
+  __syncthreads();
+  // 5. time-domain blocks (rows of BW floats, left in the tiles with a pitch of NH complex)
+  constexpr int HALF = BW / 2;
+  for (int i = t; i < count * BH * HALF; i += NT) {
+    const int j = i / (BH * HALF), r = i - j * (BH * HALF);
+    const int y = r / HALF, x = r - y * HALF;
+    reinterpret_cast<float2*>(ts.tdom[j] + (size_t)blockIdx.x * BH * BW)[r] = S[j * BINS + y * NH + x];
   }
 }
 
@@ -1114,10 +1433,35 @@ template <int BW, int BH>
 cudaError_t inv_frames(const InverseArgs& a, const FrameSet& fs, int mode, cudaStream_t s) {
   if (fs.count < 1 || fs.count > kMaxGroupFrames) return cudaErrorInvalidValue;
   switch (mode) {
+    case MODE_SHARPEN_ONLY: return inv_frames_mode<BW, BH, MODE_SHARPEN_ONLY>(a, fs, s);
     case 2: return inv_frames_mode<BW, BH, 2>(a, fs, s);
     case 3: return inv_frames_mode<BW, BH, 3>(a, fs, s);
     case 4: return inv_frames_mode<BW, BH, 4>(a, fs, s);
     case 5: return inv_frames_mode<BW, BH, 5>(a, fs, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <int BW, int BH, int MODE>
+cudaError_t inv_group_mode(const InverseArgs& a, const TemporalSet& ts, cudaStream_t s) {
+  const int smem = group_smem_bytes<BW, BH>(kGroupTile);
+  cudaError_t e = fft3d::smem_attr(k_filter_inverse_group<BW, BH, MODE>, smem);
+  if (e != cudaSuccess) return e;
+  k_filter_inverse_group<BW, BH, MODE><<<a.g.nblocks, kWarps * 32, group_smem_bytes<BW, BH>(ts.count), s>>>(a, ts);
+  return cudaGetLastError();
+}
+
+template <int BW, int BH>
+cudaError_t inv_group(const InverseArgs& a, const TemporalSet& ts, int mode, cudaStream_t s) {
+  if (ts.count < 1 || ts.count > kGroupTile) return cudaErrorInvalidValue;
+  switch (mode) {
+    case MODE_SHARPEN_ONLY: return inv_group_mode<BW, BH, MODE_SHARPEN_ONLY>(a, ts, s);
+    case MODE_KALMAN: return inv_group_mode<BW, BH, MODE_KALMAN>(a, ts, s);
+    case 1: return inv_group_mode<BW, BH, 1>(a, ts, s);
+    case 2: return inv_group_mode<BW, BH, 2>(a, ts, s);
+    case 3: return inv_group_mode<BW, BH, 3>(a, ts, s);
+    case 4: return inv_group_mode<BW, BH, 4>(a, ts, s);
+    case 5: return inv_group_mode<BW, BH, 5>(a, ts, s);
   }
   return cudaErrorInvalidValue;
 }
@@ -1143,6 +1487,6 @@ cudaError_t inv_sized(const InverseArgs& a, int mode, cudaStream_t s) {
   static const bool fft3d_reg_##BW##x##BH = register_size(                                             \
       SizeEntry{BW, BH, &fwd_sized<BW, BH>, &inv_sized<BW, BH>, &fused_sized<BW, BH>, &upload_twiddle_table, \
                 &fwd_batch<BW, BH>, &inv_batch<BW, BH>, &ctas_per_plane<BW, BH>, &occupancy_of<BW, BH>,      \
-                &inv_frames<BW, BH>, &fwd_frames<BW, BH>});
+                &inv_frames<BW, BH>, &fwd_frames<BW, BH>, &inv_group<BW, BH>});
 
 }  // namespace fft3d

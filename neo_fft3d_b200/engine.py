@@ -14,7 +14,8 @@ import numpy as np
 from .params import FFT3DParams, PlaneDesc, make_params, plane_descs, processed_planes
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "libfft3d_b200.so")
+# NEO_FFT3D_LIB: another build of the same library (A/B measurements)
+LIB_PATH = os.environ.get("NEO_FFT3D_LIB") or os.path.join(_HERE, "lib", "libfft3d_b200.so")
 _lib = None
 
 SYMBOLS = ("fft3d_params_default", "fft3d_plane_create", "fft3d_plane_filter", "fft3d_plane_filter_device",
