@@ -403,12 +403,13 @@ __device__ __forceinline__ BinTab bin_tab(const InverseArgs& a, int bin) {
 __device__ __forceinline__ float bin_psd(float re, float im) { return fmaf(re, re, fmaf(im, im, 1.0e-15f)); }
 
 __device__ __forceinline__ float sharpen_fact(const InverseArgs& a, float psd, float wsh) {
-  // src/code_impl/Apply.cpp:129-131: 1 + sharpen * wsh * sqrt(N / D) with
-  // N = psd * smax2n, D = (psd + smin2n)(psd + smax2n), evaluated as
-  // N * rsqrt(N * D) (N = 0 when smax = 0: the clamp keeps 0 * rsqrt finite)
-  const float n = psd * a.c.smax2n;
-  const float d = (psd + a.c.smin2n) * (psd + a.c.smax2n);
-  return fmaf(a.c.sharpen * wsh, n * rsqrtf(fmaxf(n * d, 1e-30f)), 1.f);
+  // src/code_impl/Apply.cpp:129-131: 1 + sharpen * wsh * sqrt(r) with
+  // r = psd * smax2n / ((psd + smin2n)(psd + smax2n)) in [0, 1), the ratio
+  // first as in the reference (the product of its terms overflows float for
+  // high bit depths), its square root as r * rsqrt(r) (the clamp keeps r = 0,
+  // i.e. smax = 0, finite)
+  const float r = __fdividef(psd * a.c.smax2n, (psd + a.c.smin2n) * (psd + a.c.smax2n));
+  return fmaf(a.c.sharpen * wsh, r * rsqrtf(fmaxf(r, 1e-30f)), 1.f);
 }
 __device__ __forceinline__ float dehalo_fact(const InverseArgs& a, float psd, float wdh) {
   // src/code_impl/Apply.cpp:132

@@ -95,3 +95,19 @@ def test_forward_spectrum(gpu, bw, bh):
         ref = restate.OraclePlane(p, d, dbl=True).spectrum(a[0])
         err = np.abs(got - ref).reshape(got.shape[0], -1).max(1) / np.abs(ref).reshape(ref.shape[0], -1).max(1)
         assert err.max() <= SPEC_TOL, (bw, bh, i, err.max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", [dict(sigma=2.0, bt=1, sharpen=0.6, dehalo=0.5),
+                                  dict(sigma=2.0, bt=3, sharpen=0.6, smax=40.0)], ids=["wiener2d", "wiener3"])
+def test_sharpen_full_range_16bit(gpu, case):
+    """Sharpen/dehalo on bright 16-bit planes: the sharpen factor's terms
+    (psd * smax^2 and (psd + smin^2)(psd + smax^2), in 16-bit units) are far
+    above 8-bit ones, so an evaluation that multiplies them overflows float."""
+    planes = synth.make_clip(176, 144, 5, bits=16, noise_sigma=4 << 8, seed=14)
+    planes = [np.minimum(a.astype(np.int64) * 5 // 4, 65535).astype(np.uint16) for a in planes]  # up to full scale
+    want = restate.filter_clip(planes, bits=16, **case)
+    got = engine.filter_clip(planes, bits=16, **case)
+    for g, w in zip(got, want):
+        mx, frac = _compare(g, w)
+        assert frac >= PIX_TOL_FRAC and mx <= 2, (case, mx, frac)
