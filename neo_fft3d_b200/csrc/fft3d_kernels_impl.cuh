@@ -499,75 +499,71 @@ __device__ __forceinline__ float2 filter_vals(const InverseArgs& a, const float2
     }
     return make_float2(cr * f + gc.x, ci * f + gc.y);
   } else {
-    // Wiener 3D over MODE frames, src/code_impl/Apply.cpp:67-235
-    // gc * bt (src/code_impl/Apply.cpp:78-93); gf * MODE is the same for every
-    // bin of the block and leaves the bin loop
+    // Wiener 3D over MODE frames, src/code_impl/Apply.cpp:67-235. The short
+    // temporal DFT works on (re, im) pairs with packed f32x2 adds and
+    // multiplies (one instruction per complex sum or real-scaled term); the
+    // terms and their signs are the reference's, the association of a few
+    // sums differs (rounding only). gc * bt (src/code_impl/Apply.cpp:78-93)
+    // uses gf * MODE, the same for every bin of the block.
     const float gk = gf * (float)MODE;
-    float g0 = 0.f, g1 = 0.f;
-    if (a.c.degrid != 0.f) {
-      g0 = gk * tb.grid.x;
-      g1 = gk * tb.grid.y;
-    }
+    float2 g = make_float2(0.f, 0.f);
+    if (a.c.degrid != 0.f) g = __fmul2_rn(tb.grid, make_float2(gk, gk));
     const float noise = a.psd ? learned_noise(a, off, bin) : a.c.pattern ? __ldg(a.t.pattern3d + bin) : a.c.sigma2n;
     const float ll = a.c.lowlimit;
-    const float cr = cur.x, ci = cur.y;
+    auto wf = [&](float2& v) { wiener(v.x, v.y, noise, ll); };
+    auto add = [](float2 x, float2 y) { return __fadd2_rn(x, y); };
+    auto sub = [](float2 x, float2 y) { return __fadd2_rn(x, make_float2(-y.x, -y.y)); };
+    auto rot = [](float2 v) { return make_float2(v.y, -v.x); };  // -i v
     if constexpr (MODE == 2) {
       const float2 pv = w[1];
-      float f0r = cr + pv.x - g0, f0i = ci + pv.y - g1;
-      float f1r = cr - pv.x, f1i = ci - pv.y;
-      wiener(f0r, f0i, noise, ll);
-      wiener(f1r, f1i, noise, ll);
-      return make_float2((f0r + f1r + g0) * 0.5f, (f0i + f1i + g1) * 0.5f);
+      float2 f0 = sub(add(cur, pv), g), f1 = sub(cur, pv);
+      wf(f0);
+      wf(f1);
+      return __fmul2_rn(add(add(f0, f1), g), make_float2(0.5f, 0.5f));
     } else if constexpr (MODE == 3) {
       const float sin120 = 0.86602540378443864676372317075294f;
       const float2 pv = w[1], nx = w[3];
-      const float pnr = pv.x + nx.x, pni = pv.y + nx.y;
-      float fcr = cr + pnr - g0, fci = ci + pni - g1;
-      const float di = sin120 * (pv.y - nx.y), dr = sin120 * (nx.x - pv.x);
-      float fpr = cr - 0.5f * pnr + di, fnr = cr - 0.5f * pnr - di;
-      float fpi = ci - 0.5f * pni + dr, fni = ci - 0.5f * pni - dr;
-      wiener(fcr, fci, noise, ll);
-      wiener(fpr, fpi, noise, ll);
-      wiener(fnr, fni, noise, ll);
+      const float2 pn = add(pv, nx);
+      float2 fc = sub(add(cur, pn), g);
+      const float2 h = __ffma2_rn(pn, make_float2(-0.5f, -0.5f), cur);      // cur - pn / 2
+      const float2 m = rot(__fmul2_rn(sub(pv, nx), make_float2(sin120, sin120)));  // (di, dr)
+      float2 fp = add(h, m), fn = sub(h, m);
+      wf(fc);
+      wf(fp);
+      wf(fn);
       const float third = 1.0f / 3.0f;
-      return make_float2((fcr + fpr + fnr + g0) * third, (fci + fpi + fni + g1) * third);
+      return __fmul2_rn(add(add(add(fc, fp), fn), g), make_float2(third, third));
     } else if constexpr (MODE == 4) {
       const float2 p2 = w[0], pv = w[1], nx = w[3];
-      float fp2r = (cr + p2.x) - (pv.x + nx.x), fp2i = (ci + p2.y) - (pv.y + nx.y);
-      float fpr = (cr - p2.x) + (pv.y - nx.y), fpi = (ci - p2.y) - (pv.x - nx.x);
-      float fcr = (cr + p2.x) + (pv.x + nx.x) - g0, fci = (ci + p2.y) + (pv.y + nx.y) - g1;
-      float fnr = (cr - p2.x) - (pv.y - nx.y), fni = (ci - p2.y) + (pv.x - nx.x);
-      wiener(fp2r, fp2i, noise, ll);
-      wiener(fpr, fpi, noise, ll);
-      wiener(fcr, fci, noise, ll);
-      wiener(fnr, fni, noise, ll);
-      return make_float2(((fp2r + fpr) + (fcr + fnr) + g0) * 0.25f, ((fp2i + fpi) + (fci + fni) + g1) * 0.25f);
+      const float2 cp = add(cur, p2), cm = sub(cur, p2), pn = add(pv, nx);
+      const float2 d = rot(sub(pv, nx));  // (pv.y - nx.y, nx.x - pv.x)
+      float2 fp2 = sub(cp, pn), fc = sub(add(cp, pn), g);
+      float2 fp = add(cm, d), fn = sub(cm, d);
+      wf(fp2);
+      wf(fp);
+      wf(fc);
+      wf(fn);
+      return __fmul2_rn(add(add(add(fp2, fp), add(fc, fn)), g), make_float2(0.25f, 0.25f));
     } else {
       const float sin72 = 0.95105651629515357211643933337938f, cos72 = 0.30901699437494742410229341718282f;
       const float sin144 = 0.58778525229247312916870595463907f, cos144 = -0.80901699437494742410229341718282f;
-      const float2 p2 = w[0], pv = w[1];
-      const float2 nx = w[3], n2 = w[4];
-      float sum = (p2.x + n2.x) * cos72 + (pv.x + nx.x) * cos144 + cr;
-      float dif = (-p2.y + n2.y) * sin72 + (pv.y - nx.y) * sin144;
-      float fp2r = sum + dif, fn2r = sum - dif;
-      sum = (p2.y + n2.y) * cos72 + (pv.y + nx.y) * cos144 + ci;
-      dif = (p2.x - n2.x) * sin72 + (-pv.x + nx.x) * sin144;
-      float fp2i = sum + dif, fn2i = sum - dif;
-      sum = (p2.x + n2.x) * cos144 + (pv.x + nx.x) * cos72 + cr;
-      dif = (p2.y - n2.y) * sin144 + (pv.y - nx.y) * sin72;
-      float fpr = sum + dif, fnr = sum - dif;
-      sum = (p2.y + n2.y) * cos144 + (pv.y + nx.y) * cos72 + ci;
-      dif = (-p2.x + n2.x) * sin144 + (-pv.x + nx.x) * sin72;
-      float fpi = sum + dif, fni = sum - dif;
-      float fcr = (p2.x + pv.x) + cr + (nx.x + n2.x) - g0;
-      float fci = (p2.y + pv.y) + ci + (nx.y + n2.y) - g1;
-      wiener(fp2r, fp2i, noise, ll);
-      wiener(fpr, fpi, noise, ll);
-      wiener(fcr, fci, noise, ll);
-      wiener(fnr, fni, noise, ll);
-      wiener(fn2r, fn2i, noise, ll);
-      return make_float2(((fp2r + fpr) + (fcr + fnr) + fn2r + g0) * 0.2f,
-                         ((fp2i + fpi) + (fci + fni) + fn2i + g1) * 0.2f);
+      const float2 p2 = w[0], pv = w[1], nx = w[3], n2 = w[4];
+      const float2 a2 = add(p2, n2), a1 = add(pv, nx);  // outer and inner pair sums
+      const float2 e2 = sub(n2, p2), e1 = sub(pv, nx);  // their differences
+      const float2 s1 = add(__ffma2_rn(a2, make_float2(cos72, cos72), __fmul2_rn(a1, make_float2(cos144, cos144))), cur);
+      const float2 s2 = add(__ffma2_rn(a2, make_float2(cos144, cos144), __fmul2_rn(a1, make_float2(cos72, cos72))), cur);
+      // -i (e2 sin72 + e1 sin144) and -i (e1 sin72 - e2 sin144)
+      const float2 t1 = rot(__ffma2_rn(e2, make_float2(sin72, sin72), __fmul2_rn(e1, make_float2(sin144, sin144))));
+      const float2 t2 = rot(__ffma2_rn(e2, make_float2(-sin144, -sin144), __fmul2_rn(e1, make_float2(sin72, sin72))));
+      float2 fp2 = add(s1, t1), fn2 = sub(s1, t1);
+      float2 fp = add(s2, t2), fn = sub(s2, t2);
+      float2 fc = sub(add(add(a2, a1), cur), g);
+      wf(fp2);
+      wf(fp);
+      wf(fc);
+      wf(fn);
+      wf(fn2);
+      return __fmul2_rn(add(add(add(add(fp2, fp), add(fc, fn)), fn2), g), make_float2(0.2f, 0.2f));
     }
   }
 }
