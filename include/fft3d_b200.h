@@ -258,9 +258,10 @@ int fft3d_batch_set_tuning(fft3d_batch* b, int enable);
 int fft3d_batch_step(fft3d_batch* b, int count, fft3d_plane* const* planes, const int* n, const void* const* src,
                      const int* src_stride, void* const* dst, const int* dst_stride, void* stream);
 
-/* out[0] steps, [1] graph launches, [2] tuning steps, [3] 0, [4] kernels
- * of the last step, [5] step shapes seen, [6] wave budget (MiB, 0 = one
- * wave) of the last tuned step, [7] 0. */
+/* out[0] steps, [1] graph launches, [2] tuning steps, [3] host milliseconds
+ * spent planning the steps' planes (summed), [4] kernels of the last step,
+ * [5] step shapes seen, [6] wave budget (MiB, 0 = one wave) of the last
+ * tuned step, [7] host milliseconds of the steps (summed). */
 int fft3d_batch_stats(fft3d_batch* b, double out[8]);
 
 /* Per-phase kernel timing (1 = on). While on, tuned steps run without their

@@ -13,15 +13,21 @@ device with the sinusoid-field formula of synth.make_clip.
 All planes are filtered per time step: (a) one plane at a time
 (fft3d_plane_filter_device, 3 launches per plane) on one stream, and (b) as
 one batched step (fft3d_batch_step: one persistent launch per kernel variant,
-phase and wave; autotuned; CUDA-graph replayed). Both passes are timed after
-a first untimed pass (which, for the batch, tunes and captures); the outputs
-of the two are compared byte for byte. Prints one JSON line.
+phase and wave; autotuned; CUDA-graph replayed). With --group G (default 8)
+the same comparison runs again in frame groups: (c) each plane's next G
+output frames per call (fft3d_plane_filter_frames_device), plane after plane
+on one stream, against (d) one batched step of G consecutive frames of every
+plane (each plane's frames run as one run of its filter/inverse with one CTA
+per block). Every pass is timed after a first untimed pass (which, for the
+batch, tunes and captures); the outputs of each pair are compared byte for
+byte. Prints one JSON line.
 """
 from __future__ import annotations
 
 import argparse
 import json
 import os
+import time
 
 import numpy as np
 
@@ -52,6 +58,10 @@ def main():
     ap.add_argument("--frames", type=int, default=60)
     ap.add_argument("--seed", type=int, default=3000)
     ap.add_argument("--mix", default="uneven", choices=sorted(MIXES))
+    ap.add_argument("--group", type=int, default=8, help="frames per plane per call/step of the grouped passes")
+    ap.add_argument("--no-tune", action="store_true", help="default schedules (one wave), no autotuning")
+    ap.add_argument("--phase-timing", action="store_true",
+                    help="one more pass of each grouped form with per-kernel timing (per-plane) / per-phase timing (batch)")
     args = ap.parse_args()
     F = args.frames
     kinds = MIXES[args.mix]
@@ -74,7 +84,9 @@ def main():
             P = a.shape[1] * a.shape[2] * a.element_size()
             canonical += 2 * P + S + max(s["bt"], 1) * S
     torch.cuda.synchronize()
-    stream = torch.cuda.current_stream()
+    # every pass on one dedicated stream, which the timing events bracket
+    # (stream 0 would mean each plane's own stream in the per-plane calls)
+    stream = torch.cuda.Stream()
 
     def item(e, a, o, n):
         fb = a.shape[1] * a.shape[2] * a.element_size()
@@ -87,11 +99,13 @@ def main():
                 _, _, ptrs, st, dst, ds = item(e, a, o, n)
                 e.filter_device(n, ptrs, st, dst, ds, stream.cuda_stream)
 
-    batch = engine.Batch(tuning=True)
+    batch = engine.Batch(tuning=not args.no_tune)
 
     def batched_pass():
         for n in range(F):
             batch.step([item(e, a, o, n) for e, a, o in zip(engs, clips, outs)], stream.cuda_stream)
+
+    host_s = {}
 
     def timed(fn):
         for e in engs:
@@ -99,10 +113,38 @@ def main():
         torch.cuda.synchronize()
         t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0.record(stream)
+        h = time.perf_counter()
         fn()
+        host_s[fn.__name__] = time.perf_counter() - h  # the host's time to issue the pass
         t1.record(stream)
         torch.cuda.synchronize()
         return t0.elapsed_time(t1) / 1000.0
+
+    G = args.group
+
+    def group_items(e, a, o, n0, k):
+        fb = a.shape[1] * a.shape[2] * a.element_size()
+        st = a.shape[2] * a.element_size()
+        return [item(e, a, o, n) for n in range(n0, n0 + k)], \
+            ([a.data_ptr() + m * fb if 0 <= m < F else 0 for m in range(n0 - 2, n0 + k + 2)], [st] * (k + 4),
+             [o.data_ptr() + n * fb for n in range(n0, n0 + k)], [st] * k)
+
+    def per_plane_grouped_pass():
+        for n0 in range(0, F, G):
+            k = min(G, F - n0)
+            for e, a, o in zip(engs, clips, outs):
+                ptrs, sts, dsts, dsts_st = group_items(e, a, o, n0, k)[1]
+                e.filter_frames_device(n0, ptrs, sts, dsts, dsts_st, stream.cuda_stream)
+
+    gbatch = engine.Batch(tuning=not args.no_tune)
+
+    def batched_grouped_pass():
+        for n0 in range(0, F, G):
+            k = min(G, F - n0)
+            its = []
+            for e, a, o in zip(engs, clips, outs):
+                its += group_items(e, a, o, n0, k)[0]
+            gbatch.step(its, stream.cuda_stream)
 
     timed(per_plane_pass)  # warm-up
     l0 = engine.kernel_launches()
@@ -115,6 +157,46 @@ def main():
     launches_batch = engine.kernel_launches() - l0
     same = all(bool(torch.equal(r, o)) for r, o in zip(ref, outs))
     stats = batch.stats()
+    grouped = None
+    if G > 1:
+        timed(per_plane_grouped_pass)
+        l0 = engine.kernel_launches()
+        t_pg = timed(per_plane_grouped_pass)
+        launches_pg = engine.kernel_launches() - l0
+        same_pg = all(bool(torch.equal(r, o)) for r, o in zip(ref, outs))
+        # tuning and capture: every step shape of the pass (clip start, middle,
+        # end) first takes its tuning steps
+        for _ in range(10):
+            before = gbatch.stats()["tuning_steps"]
+            timed(batched_grouped_pass)
+            if gbatch.stats()["tuning_steps"] == before:
+                break
+        l0 = engine.kernel_launches()
+        t_bg = timed(batched_grouped_pass)
+        launches_bg = engine.kernel_launches() - l0
+        same_bg = all(bool(torch.equal(r, o)) for r, o in zip(ref, outs))
+        phases = None
+        if args.phase_timing:
+            for e in engs:
+                e.set_timing(True)
+            timed(per_plane_grouped_pass)
+            per = {}
+            for e in engs:
+                for k, (n, ms, _) in e.timing().items():
+                    per[k] = per.get(k, 0.0) + ms
+                e.set_timing(False)
+            gbatch.set_timing(True)
+            timed(batched_grouped_pass)
+            bt_ = gbatch.timing()
+            gbatch.set_timing(False)
+            phases = dict(per_plane_ms_per_pass={k: v for k, v in per.items() if v > 0},
+                          batched_ms_per_pass={k: v[1] for k, v in bt_.items()})
+        grouped = dict(frames_per_call=G, phase_timing=phases,
+                       stream_frames_per_s=dict(per_plane=len(cfg) * F / t_pg, batched=len(cfg) * F / t_bg),
+                       speedup=t_pg / t_bg,
+                       kernels_per_frame=dict(per_plane=launches_pg / F, batched=launches_bg / F),
+                       outputs_identical_to_one_frame_per_call=dict(per_plane=same_pg, batched=same_bg),
+                       batch_stats=gbatch.stats())
     peak = None
     peaks = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "MEASURED_PEAKS.json")
     if os.path.exists(peaks):
@@ -134,7 +216,16 @@ def main():
                 bw_counts={str(k): sum(1 for s in cfg if s["bw"] == k) for k in (32, 48)})
     if peak:
         line["hbm_frac"] = {k: v / peak for k, v in line["hbm_gbs"].items()}
+    line["host_issue_s_per_pass"] = dict(per_plane=host_s.get("per_plane_pass"), batched=host_s.get("batched_pass"))
+    if grouped:
+        grouped["hbm_gbs"] = {k: canonical * v / len(cfg) / 1e9 for k, v in grouped["stream_frames_per_s"].items()}
+        grouped["host_issue_s_per_pass"] = dict(per_plane=host_s.get("per_plane_grouped_pass"),
+                                                batched=host_s.get("batched_grouped_pass"))
+        if peak:
+            grouped["hbm_frac"] = {k: v / peak for k, v in grouped["hbm_gbs"].items()}
+        line["frame_groups"] = grouped
     print(json.dumps(line), flush=True)
+    gbatch.close()
     batch.close()
     for e in engs:
         e.close()

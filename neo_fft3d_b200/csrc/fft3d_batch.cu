@@ -29,6 +29,7 @@
 // graph instances alternate over two staging buffers so that the host can
 // prepare a step while the previous one runs.
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -121,16 +122,20 @@ struct Captured {
   }
 };
 
-size_t arg_size(int phase) {
+// filter/inverse groups whose var is kRunVar + mode launch runs of frame groups
+constexpr int kRunVar = 100;
+
+size_t arg_size(int phase, int var) {
   switch (phase) {
     case PH_FWD: return sizeof(fft3d::ForwardArgs);
-    case PH_INV: return sizeof(fft3d::InverseArgs);
+    case PH_INV: return var >= kRunVar ? sizeof(fft3d::GroupRun) : sizeof(fft3d::InverseArgs);
     case PH_COPY: return sizeof(fft3d::CopyArgs);
     default: return sizeof(fft3d::OlaArgs);
   }
 }
 
-const fft3d::Geom& rec_geom(const Deferred& d, int phase, int r) {
+const fft3d::Geom& rec_geom(const Deferred& d, int phase, int var, int r) {
+  if (phase == PH_INV && var >= kRunVar) return d.runs[r].r.a.g;
   return phase == PH_FWD ? d.fwd[r].a.g : (phase == PH_INV ? d.inv[r].a.g : d.ola[r].a.g);
 }
 
@@ -160,8 +165,10 @@ struct fft3d_batch {
   void* h_direct = nullptr;
   size_t h_direct_cap = 0;
   cudaEvent_t direct_done = nullptr;
-  double stats[8] = {};  // steps, graph launches, tuning steps, -, kernels of the last step, step shapes,
-                         // wave budget (MiB) of the last tuned step
+  // steps, graph launches, tuning steps, host ms planning the planes (sum),
+  // kernels of the last step, step shapes, wave budget (MiB) of the last
+  // tuned step, host ms of the steps (sum)
+  double stats[8] = {};
   // optional per-phase timing: tuned steps run without the graph, with
   // events around each launch, resolved when the counters are read
   struct Pending {
@@ -176,10 +183,10 @@ struct fft3d_batch {
 
 namespace {
 
-int rec_plane(const Deferred& d, int phase, int r) {
+int rec_plane(const Deferred& d, int phase, int var, int r) {
   switch (phase) {
     case PH_FWD: return d.fwd[r].plane;
-    case PH_INV: return d.inv[r].plane;
+    case PH_INV: return var >= kRunVar ? d.runs[r].plane : d.inv[r].plane;
     case PH_COPY: return d.copies[r].plane;
     default: return d.ola[r].plane;
   }
@@ -192,11 +199,16 @@ void build_groups(const Deferred& d, int nplanes, size_t budget, Plan& plan) {
     const fft3d::Geom& g = r.a.g;
     weight[r.plane] += (double)g.nblocks * g.bh * (g.bw / 2 + 1) * 8 + (double)g.nblocks * g.bh * g.bw * 4;
   }
+  // a run's frames count against the wave of its first plane item
+  for (const auto& r : d.runs)
+    for (int k = 1; k < r.r.ts.count; k++) weight[r.plane] += weight[r.plane + k], weight[r.plane + k] = 0.0;
   std::vector<int> wave(nplanes, 0);
   int w = 0;
   double acc = 0.0;
   for (int p = 0; p < nplanes; p++) {
-    if (budget && acc > 0.0 && acc + weight[p] > (double)budget) {
+    // an item whose work is merged into an earlier item's run (weight 0)
+    // stays in that item's wave: the run reads the spectra it transforms
+    if (budget && weight[p] > 0.0 && acc > 0.0 && acc + weight[p] > (double)budget) {
       w++;
       acc = 0.0;
     }
@@ -205,7 +217,7 @@ void build_groups(const Deferred& d, int nplanes, size_t budget, Plan& plan) {
   }
   std::map<std::tuple<int, int, int, int, int>, int> index;
   auto add = [&](int phase, int r, int bw, int bh, int var) {
-    const int wv = wave[rec_plane(d, phase, r)];
+    const int wv = wave[rec_plane(d, phase, var, r)];
     auto key = std::make_tuple(wv, phase, bw, bh, var);
     auto it = index.find(key);
     int gi;
@@ -225,16 +237,25 @@ void build_groups(const Deferred& d, int nplanes, size_t budget, Plan& plan) {
     Group& g = plan.groups[gi];
     int items;
     if (phase == PH_COPY) items = (int)d.copies[r].height;
-    else if (phase == PH_OLA) items = fft3d::batch_items_overlap_add(rec_geom(d, phase, r));
-    else items = fft3d::batch_items_forward(rec_geom(d, phase, r));
+    else if (phase == PH_OLA)
+      items = var >= fft3d::kOla4Var ? fft3d::batch_items_overlap_add4(rec_geom(d, phase, var, r))
+                                     : fft3d::batch_items_overlap_add(rec_geom(d, phase, var, r));
+    else if (phase == PH_INV && var >= kRunVar) items = d.runs[r].r.a.g.nblocks;  // one CTA per block
+    else items = fft3d::batch_items_forward(rec_geom(d, phase, var, r));
     g.recs.push_back(r);
     g.per.push_back(items);
     g.nitems += items;
   };
   for (int r = 0; r < (int)d.fwd.size(); r++) add(PH_FWD, r, d.fwd[r].a.g.bw, d.fwd[r].a.g.bh, d.fwd[r].bytes);
-  for (int r = 0; r < (int)d.inv.size(); r++) add(PH_INV, r, d.inv[r].a.g.bw, d.inv[r].a.g.bh, d.inv[r].mode);
+  for (int r = 0; r < (int)d.inv.size(); r++)
+    if (d.inv_in_run.empty() || !d.inv_in_run[r]) add(PH_INV, r, d.inv[r].a.g.bw, d.inv[r].a.g.bh, d.inv[r].mode);
+  for (int r = 0; r < (int)d.runs.size(); r++)
+    add(PH_INV, r, d.runs[r].r.a.g.bw, d.runs[r].r.a.g.bh, kRunVar + d.runs[r].mode);
   for (int r = 0; r < (int)d.copies.size(); r++) add(PH_COPY, r, 0, 0, 0);
-  for (int r = 0; r < (int)d.ola.size(); r++) add(PH_OLA, r, 0, 0, d.ola[r].bytes);
+  // overlap-adds: the 4-pixel form for planes that meet its rules
+  for (int r = 0; r < (int)d.ola.size(); r++)
+    add(PH_OLA, r, 0, 0,
+        d.ola[r].bytes + (fft3d::batch_overlap_add4_ok(d.ola[r].a, d.ola[r].bytes) ? fft3d::kOla4Var : 0));
   // waves in order, phases in order within a wave; the larger groups first
   std::stable_sort(plan.groups.begin(), plan.groups.end(), [](const Group& a, const Group& b) {
     if (a.wave != b.wave) return a.wave < b.wave;
@@ -243,7 +264,7 @@ void build_groups(const Deferred& d, int nplanes, size_t budget, Plan& plan) {
   std::string sig;
   size_t off = 0;
   for (auto& g : plan.groups) {
-    g.arg_size = arg_size(g.phase);
+    g.arg_size = arg_size(g.phase, g.var);
     g.args_off = off;
     off = align_up(off + g.arg_size * g.recs.size(), 256);
     sig += std::to_string(g.wave) + "/" + std::to_string(g.phase) + "/" + std::to_string(g.bw) + "x" +
@@ -271,7 +292,8 @@ void write_args(const Deferred& d, const Plan& plan, char* base) {
         continue;
       }
       const void* src = g.phase == PH_FWD ? (const void*)&d.fwd[r].a
-                                          : (g.phase == PH_INV ? (const void*)&d.inv[r].a : (const void*)&d.ola[r].a);
+                        : g.phase == PH_INV ? (g.var >= kRunVar ? (const void*)&d.runs[r].r : (const void*)&d.inv[r].a)
+                                            : (const void*)&d.ola[r].a;
       std::memcpy(p + i * g.arg_size, src, g.arg_size);
     }
   }
@@ -304,6 +326,16 @@ double group_bytes(const Deferred& d, const Group& g) {
     if (g.phase == PH_FWD) {
       const fft3d::Geom& q = d.fwd[r].a.g;
       bytes += (double)q.W * q.H * d.fwd[r].bytes + (double)q.nblocks * q.bh * q.nh * 8;
+    } else if (g.phase == PH_INV && g.var >= kRunVar) {
+      const fft3d::GroupRun& u = d.runs[r].r;
+      const double S = (double)u.a.g.nblocks * u.a.g.bh * u.a.g.nh * 8;
+      for (const float2* p : u.ts.spec)
+        if (p && std::find(seen.begin(), seen.end(), (const void*)p) == seen.end()) {
+          seen.push_back(p);
+          bytes += S;
+        }
+      bytes += (double)u.ts.count * u.a.g.nblocks * u.a.g.bh * u.a.g.bw * 4;
+      if (d.runs[r].mode == 0) bytes += 2.0 * S * 2;
     } else if (g.phase == PH_INV) {
       const fft3d::InverseArgs& a = d.inv[r].a;
       const double S = (double)a.g.nblocks * a.g.bh * a.g.nh * 8;
@@ -333,7 +365,7 @@ void interleave_all(Plan& plan) {
 
 void set_grids(fft3d_batch* b, Plan& plan) {
   for (auto& g : plan.groups) {
-    const int which = g.phase;
+    const int which = g.phase == PH_FWD ? 0 : g.phase == PH_INV ? (g.var >= kRunVar ? 3 : 1) : g.phase == PH_OLA ? 2 : 4;
     g.occupancy = fft3d::batch_occupancy(g.bw, g.bh, which, g.var);
     const int per_sm = g.sched.per_sm == 0 ? 0 : std::min(g.sched.per_sm, g.occupancy);
     g.grid = per_sm == 0 ? g.nitems : std::max(1, std::min(g.nitems, per_sm * b->sms));
@@ -347,6 +379,8 @@ cudaError_t launch_group(const Group& g, const char* d_base, cudaStream_t s) {
   l.nitems = g.nitems;
   l.grid = g.grid;
   if (g.phase == PH_FWD) return fft3d::launch_forward_batch(g.bw, g.bh, l, g.var, s);
+  if (g.phase == PH_INV && g.var >= kRunVar)
+    return fft3d::launch_filter_inverse_group_batch(g.bw, g.bh, l, g.var - kRunVar, s);
   if (g.phase == PH_INV) return fft3d::launch_filter_inverse_batch(g.bw, g.bh, l, g.var, s);
   if (g.phase == PH_COPY) return fft3d::launch_copy_batch(l, s);
   return fft3d::launch_overlap_add_batch(l, g.var, s);
@@ -472,6 +506,13 @@ int fft3d_batch_step(fft3d_batch* b, int count, fft3d_plane* const* planes, cons
   if (!b || count <= 0 || !planes || !n || !src || !src_stride || !dst || !dst_stride)
     return fft3d::engine_fail(FFT3D_E_PARAM, "neo_fft3d: invalid batch step arguments");
   std::lock_guard<std::mutex> lk(b->mu);
+  using Clock = std::chrono::steady_clock;
+  const auto t_step = Clock::now();
+  struct StepClock {
+    double& acc;
+    Clock::time_point t0;
+    ~StepClock() { acc += std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
+  } step_clock{b->stats[7], t_step};
   cudaSetDevice(b->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   // A plane may appear several times with consecutive frames (a frame
@@ -519,6 +560,7 @@ int fft3d_batch_step(fft3d_batch* b, int count, fft3d_plane* const* planes, cons
       for (auto* P : planes) fft3d::plane_mark_work(P, s);
     }
   } mark_on_exit{order, s};
+  const auto t_plan = Clock::now();
   for (int i = 0; i < count; i++) {
     d.plane = i;
     const fft3d::FrameGroup& g = groups[planes[i]];
@@ -528,6 +570,33 @@ int fft3d_batch_step(fft3d_batch* b, int count, fft3d_plane* const* planes, cons
       for (auto* P : order) fft3d::plane_discard(P, d);
       return rc;
     }
+  }
+  b->stats[3] += std::chrono::duration<double, std::milli>(Clock::now() - t_plan).count();
+  // Frame groups: the consecutive filter/inverse records of one plane and
+  // mode become runs, each launched with one CTA per block for all its
+  // frames (each window spectrum read once per run).
+  d.inv_in_run.assign(d.inv.size(), 0);
+  for (size_t i = 0; i < d.inv.size();) {
+    size_t e = i + 1;
+    while (e < d.inv.size() && planes[d.inv[e].plane] == planes[d.inv[i].plane] && d.inv[e].mode == d.inv[i].mode &&
+           d.inv[e].plane == d.inv[e - 1].plane + 1 && (int)(e - i) < fft3d::kGroupTile)
+      e++;
+    if (e - i >= 2) {
+      Deferred::Run run{};
+      run.mode = d.inv[i].mode;
+      run.plane = d.inv[i].plane;
+      run.r.a = d.inv[i].a;
+      for (auto& p : run.r.a.in) p = nullptr;
+      run.r.ts.count = (int)(e - i);
+      for (size_t k = i; k < e; k++) {
+        for (int w = 0; w < 5; w++)
+          if (d.inv[k].a.in[w]) run.r.ts.spec[(k - i) + w] = d.inv[k].a.in[w];
+        run.r.ts.tdom[k - i] = d.inv[k].a.tdom;
+        d.inv_in_run[k] = 1;
+      }
+      d.runs.push_back(run);
+    }
+    i = e;
   }
   cudaSetDevice(b->device);
   Plan shape;  // the step's shape (one wave) keys its tuning

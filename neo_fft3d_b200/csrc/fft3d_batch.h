@@ -19,11 +19,16 @@ struct Deferred {
   struct Inv { InverseArgs a; int mode; int plane; };
   struct Ola { OlaArgs a; int bytes; int plane; };
   struct Copy { void* dst; size_t dpitch; const void* src; size_t spitch; size_t width; size_t height; int plane; };
+  // consecutive filter/inverse records of one plane and mode (a frame group's
+  // run) merged into one work list: one CTA per block for all its frames
+  struct Run { GroupRun r; int mode; int plane; };
   int plane = 0;  // index of the plane being planned (tags the records)
   std::vector<Fwd> fwd;
   std::vector<Inv> inv;
   std::vector<Ola> ola;
   std::vector<Copy> copies;  // device-to-device, before the overlap-add phase
+  std::vector<Run> runs;
+  std::vector<char> inv_in_run;  // per inv record: covered by a run
 };
 
 // Consecutive output frames n0 .. n0 + count - 1 of one plane planned into

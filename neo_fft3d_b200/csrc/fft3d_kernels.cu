@@ -225,6 +225,21 @@ __global__ void __launch_bounds__(kOlaTx * kOlaTy) k_overlap_add_batch(const Ola
   }
 }
 
+// Batched 4-pixel overlap-add: work item = (plane, 128x8-pixel tile); every
+// plane of the launch meets the 4-pixel kernel's geometry and alignment rules
+// (batch_overlap_add4_ok).
+template <typename T>
+__global__ void __launch_bounds__(kOlaTx * kOlaTy) k_overlap_add4_batch(const OlaArgs* __restrict__ args,
+                                                                       const int2* __restrict__ items, int nitems) {
+  for (int i = blockIdx.x; i < nitems; i += gridDim.x) {
+    const int2 it = items[i];
+    const OlaArgs a = args[it.x];  // private copy: fields stay in registers
+    const int tx = (a.g.W + 4 * kOlaTx - 1) / (4 * kOlaTx);
+    const int ty = it.y / tx, t = it.y - ty * tx;
+    overlap_add_px4<T>(a, 4 * (t * kOlaTx + threadIdx.x), ty * kOlaTy + threadIdx.y);
+  }
+}
+
 }  // namespace
 
 bool register_size(const SizeEntry& e) {
@@ -331,9 +346,21 @@ cudaError_t launch_filter_inverse_batch(int bw, int bh, const BatchLaunch& l, in
   return e ? e->inv_batch(l, mode, s) : cudaErrorInvalidValue;
 }
 
+cudaError_t launch_filter_inverse_group_batch(int bw, int bh, const BatchLaunch& l, int mode, cudaStream_t s) {
+  const SizeEntry* e = find_size(bw, bh);
+  return e ? e->inv_group_batch(l, mode, s) : cudaErrorInvalidValue;
+}
+
 cudaError_t launch_overlap_add_batch(const BatchLaunch& l, int bytes, cudaStream_t s) {
   dim3 block(kOlaTx, kOlaTy);
   const auto* args = static_cast<const OlaArgs*>(l.args);
+  if (bytes >= kOla4Var) {  // the 4-pixel form
+    bytes -= kOla4Var;
+    if (bytes == 1) k_overlap_add4_batch<uint8_t><<<l.grid, block, 0, s>>>(args, l.items, l.nitems);
+    else if (bytes == 2) k_overlap_add4_batch<uint16_t><<<l.grid, block, 0, s>>>(args, l.items, l.nitems);
+    else k_overlap_add4_batch<float><<<l.grid, block, 0, s>>>(args, l.items, l.nitems);
+    return cudaGetLastError();
+  }
   if (bytes == 1) k_overlap_add_batch<uint8_t><<<l.grid, block, 0, s>>>(args, l.items, l.nitems);
   else if (bytes == 2) k_overlap_add_batch<uint16_t><<<l.grid, block, 0, s>>>(args, l.items, l.nitems);
   else k_overlap_add_batch<float><<<l.grid, block, 0, s>>>(args, l.items, l.nitems);
@@ -401,8 +428,18 @@ int batch_items_overlap_add(const Geom& g) {
   return ((g.W + kOlaTx - 1) / kOlaTx) * ((g.H + kOlaTy - 1) / kOlaTy);
 }
 
+int batch_items_overlap_add4(const Geom& g) {
+  return ((g.W + 4 * kOlaTx - 1) / (4 * kOlaTx)) * ((g.H + kOlaTy - 1) / kOlaTy);
+}
+
+bool batch_overlap_add4_ok(const OlaArgs& a, int bytes) {
+  return a.g.sx % 4 == 0 && a.g.ow % 4 == 0 && a.g.W % 4 == 0 && a.g.bw % 4 == 0 &&
+         reinterpret_cast<uintptr_t>(a.tdom) % 16 == 0 && reinterpret_cast<uintptr_t>(a.dst) % (4 * bytes) == 0 &&
+         a.dst_stride % (4 * bytes) == 0;
+}
+
 int batch_occupancy(int bw, int bh, int which, int mode_or_bytes) {
-  if (which == 3) return 8;  // plane copies
+  if (which == 4) return 8;  // plane copies
   if (which == 2) {
     int n = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_overlap_add_batch<uint8_t>, kOlaTx * kOlaTy, 0);

@@ -129,6 +129,12 @@ struct TemporalSet {
   int count;
 };
 
+// One run of a batched step's frame groups (work items: its plane's blocks).
+struct GroupRun {
+  InverseArgs a;
+  TemporalSet ts;
+};
+
 // The new frames of a frame group, transformed by one launch: frame j's
 // samples (src/stride as in ForwardArgs) and ring slot. ctas: CTAs per frame
 // (set by the launcher).
@@ -213,10 +219,18 @@ bool overlap_add_frames_supported(const OlaArgs& a, const OlaFrameSet& fs, int b
 cudaError_t launch_forward_batch(int bw, int bh, const BatchLaunch& l, int bytes_per_sample, cudaStream_t s);
 cudaError_t launch_filter_inverse_batch(int bw, int bh, const BatchLaunch& l, int mode, cudaStream_t s);
 cudaError_t launch_overlap_add_batch(const BatchLaunch& l, int bytes_per_sample, cudaStream_t s);
+// Runs of frame groups of many planes (args: GroupRun[]; items: (run, block)).
+cudaError_t launch_filter_inverse_group_batch(int bw, int bh, const BatchLaunch& l, int mode, cudaStream_t s);
 cudaError_t launch_copy_batch(const BatchLaunch& l, cudaStream_t s);  // items: (copy, row)
 int batch_items_forward(const Geom& g);     // forward / filter-inverse work items of a plane
 int batch_items_overlap_add(const Geom& g);  // overlap-add work items (tiles) of a plane
-int batch_occupancy(int bw, int bh, int which, int mode_or_bytes);  // which: 0 fwd, 1 inv, 2 ola
+// The 4-pixel batched overlap-add (launch_overlap_add_batch with bytes +
+// kOla4Var): its work items per plane, and whether a plane meets its rules.
+constexpr int kOla4Var = 10;
+int batch_items_overlap_add4(const Geom& g);
+bool batch_overlap_add4_ok(const OlaArgs& a, int bytes_per_sample);
+// which: 0 forward, 1 filter/inverse, 2 overlap-add, 3 group runs, 4 plane copies
+int batch_occupancy(int bw, int bh, int which, int mode_or_bytes);
 // Streaming filter of all bins (Wiener 2D/3D, Kalman) into F; the sharpen pass
 // and the inverse follow with launch_filter_inverse(MODE_SHARPEN_ONLY) on F.
 cudaError_t launch_filter_bins(const InverseArgs& a, float2* F, int mode, cudaStream_t s);

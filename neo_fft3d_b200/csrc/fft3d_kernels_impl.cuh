@@ -366,13 +366,21 @@ __global__ void __launch_bounds__(kWarps * 32, 5) k_forward_frames(ForwardArgs a
 // Batched forward: work item i = (plane, CTA of that plane); the grid walks
 // the items (persistent when the grid is smaller than the item count).
 template <int BW, int BH, typename T>
-__global__ void __launch_bounds__(kWarps * 32) k_forward_batch(const ForwardArgs* __restrict__ args,
-                                                              const int2* __restrict__ items, int nitems) {
+__global__ void __launch_bounds__(kWarps * 32, 5) k_forward_batch(const ForwardArgs* __restrict__ args,
+                                                                 const int2* __restrict__ items, int nitems) {
+  // the item's arguments staged in shared memory: the body's stores cannot
+  // alias them, they cost no registers, and the body can take the per-plane
+  // kernel's row prefetch (x window read from the staged arguments)
+  __shared__ __align__(16) ForwardArgs sa;
+  static_assert(sizeof(ForwardArgs) % 4 == 0, "word copy");
   for (int i = blockIdx.x; i < nitems; i += gridDim.x) {
     const int2 it = items[i];
-    // a private copy: the body's stores cannot alias it, so its fields stay in registers
-    const ForwardArgs a = args[it.x];
-    forward_cta<BW, BH, T, false>(a, it.y);
+    __syncthreads();  // every warp is done with the previous item's arguments
+    const int* src = reinterpret_cast<const int*>(args + it.x);
+    int* dst = reinterpret_cast<int*>(&sa);
+    for (int w = threadIdx.x; w < (int)(sizeof(ForwardArgs) / 4); w += blockDim.x) dst[w] = src[w];
+    __syncthreads();
+    forward_cta<BW, BH, T, true>(sa, it.y);
   }
 }
 
@@ -1030,8 +1038,7 @@ __device__ __forceinline__ void group_filter_one(const InverseArgs& a, const Tem
 }
 
 template <int BW, int BH, int MODE>
-__global__ void __launch_bounds__(kWarps * 32, 5) k_filter_inverse_group(InverseArgs a,
-                                                                     const __grid_constant__ TemporalSet ts) {
+__device__ __forceinline__ void filter_inverse_group_cta(const InverseArgs& a, const TemporalSet& ts, int blk) {
   constexpr int NH = BW / 2 + 1, HC = BW / 2, BINS = BH * NH, PAIRS = BINS / 2, NT = kWarps * 32;
   static_assert(BINS % 2 == 0, "bin pairs");
   extern __shared__ float2 smem2[];
@@ -1039,7 +1046,7 @@ __global__ void __launch_bounds__(kWarps * 32, 5) k_filter_inverse_group(Inverse
   float* gsh = gfs + kGroupTile;                 // ... and of its filtered block (sharpen pass)
   float2* S = smem2 + kGroupTile;                // [count][BINS] tiles, 16-byte aligned
   const int count = ts.count;
-  const size_t off = (size_t)blockIdx.x * BINS;
+  const size_t off = (size_t)blk * BINS;
   const float gs0 = __ldg(&a.t.grid[0].x);
   const int t = threadIdx.x;
   // 0. grid fraction of each frame's block (its DC)
@@ -1108,7 +1115,35 @@ __global__ void __launch_bounds__(kWarps * 32, 5) k_filter_inverse_group(Inverse
   for (int i = t; i < count * BH * HALF; i += NT) {
     const int j = i / (BH * HALF), r = i - j * (BH * HALF);
     const int y = r / HALF, x = r - y * HALF;
-    reinterpret_cast<float2*>(ts.tdom[j] + (size_t)blockIdx.x * BH * BW)[r] = S[j * BINS + y * NH + x];
+    reinterpret_cast<float2*>(ts.tdom[j] + (size_t)blk * BH * BW)[r] = S[j * BINS + y * NH + x];
+  }
+}
+
+template <int BW, int BH, int MODE>
+__global__ void __launch_bounds__(kWarps * 32, 5) k_filter_inverse_group(InverseArgs a,
+                                                                     const __grid_constant__ TemporalSet ts) {
+  filter_inverse_group_cta<BW, BH, MODE>(a, ts, blockIdx.x);
+}
+
+// Batched runs of many planes: work item (run, block of that run's plane). The
+// run's arguments are staged in shared memory behind the tiles, so the body's
+// stores cannot alias them (a reference into global memory would be reloaded
+// after every store) and they cost no registers.
+template <int BW, int BH, int MODE>
+__global__ void __launch_bounds__(kWarps * 32, 5) k_filter_inverse_group_batch(const GroupRun* __restrict__ runs,
+                                                                           const int2* __restrict__ items,
+                                                                           int nitems) {
+  extern __shared__ float2 smem2[];
+  GroupRun* sr = reinterpret_cast<GroupRun*>(smem2 + kGroupTile + kGroupTile * BH * (BW / 2 + 1));
+  static_assert(sizeof(GroupRun) % 4 == 0, "word copy");
+  for (int i = blockIdx.x; i < nitems; i += gridDim.x) {
+    const int2 it = items[i];
+    __syncthreads();  // every thread is done with the previous item's arguments and tiles
+    const int* src = reinterpret_cast<const int*>(runs + it.x);
+    int* dst = reinterpret_cast<int*>(sr);
+    for (int w = threadIdx.x; w < (int)(sizeof(GroupRun) / 4); w += blockDim.x) dst[w] = src[w];
+    __syncthreads();
+    filter_inverse_group_cta<BW, BH, MODE>(sr->a, sr->ts, it.y);
   }
 }
 
@@ -1304,6 +1339,10 @@ int occupancy_of(int which, int mode_or_bytes) {
   int n = 0;
   if (which == 0) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_forward_batch<BW, BH, uint8_t>, kWarps * 32, smem);
+  } else if (which == 3) {
+    const int gsmem = group_smem_bytes<BW, BH>(kGroupTile) + (int)sizeof(GroupRun);
+    fft3d::smem_attr(k_filter_inverse_group_batch<BW, BH, 5>, gsmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_filter_inverse_group_batch<BW, BH, 5>, kWarps * 32, gsmem);
   } else {
     switch (mode_or_bytes) {
       case MODE_KALMAN:
@@ -1463,6 +1502,30 @@ cudaError_t inv_group(const InverseArgs& a, const TemporalSet& ts, int mode, cud
   return cudaErrorInvalidValue;
 }
 
+template <int BW, int BH, int MODE>
+cudaError_t inv_group_batch_mode(const BatchLaunch& l, cudaStream_t s) {
+  const int smem = group_smem_bytes<BW, BH>(kGroupTile) + (int)sizeof(GroupRun);
+  cudaError_t e = fft3d::smem_attr(k_filter_inverse_group_batch<BW, BH, MODE>, smem);
+  if (e != cudaSuccess) return e;
+  k_filter_inverse_group_batch<BW, BH, MODE><<<l.grid, kWarps * 32, smem, s>>>(static_cast<const GroupRun*>(l.args),
+                                                                             l.items, l.nitems);
+  return cudaGetLastError();
+}
+
+template <int BW, int BH>
+cudaError_t inv_group_batch(const BatchLaunch& l, int mode, cudaStream_t s) {
+  switch (mode) {
+    case MODE_SHARPEN_ONLY: return inv_group_batch_mode<BW, BH, MODE_SHARPEN_ONLY>(l, s);
+    case MODE_KALMAN: return inv_group_batch_mode<BW, BH, MODE_KALMAN>(l, s);
+    case 1: return inv_group_batch_mode<BW, BH, 1>(l, s);
+    case 2: return inv_group_batch_mode<BW, BH, 2>(l, s);
+    case 3: return inv_group_batch_mode<BW, BH, 3>(l, s);
+    case 4: return inv_group_batch_mode<BW, BH, 4>(l, s);
+    case 5: return inv_group_batch_mode<BW, BH, 5>(l, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
 template <int BW, int BH>
 cudaError_t inv_sized(const InverseArgs& a, int mode, cudaStream_t s) {
   switch (mode) {
@@ -1484,6 +1547,6 @@ cudaError_t inv_sized(const InverseArgs& a, int mode, cudaStream_t s) {
   static const bool fft3d_reg_##BW##x##BH = register_size(                                             \
       SizeEntry{BW, BH, &fwd_sized<BW, BH>, &inv_sized<BW, BH>, &fused_sized<BW, BH>, &upload_twiddle_table, \
                 &fwd_batch<BW, BH>, &inv_batch<BW, BH>, &ctas_per_plane<BW, BH>, &occupancy_of<BW, BH>,      \
-                &inv_frames<BW, BH>, &fwd_frames<BW, BH>, &inv_group<BW, BH>});
+                &inv_frames<BW, BH>, &fwd_frames<BW, BH>, &inv_group<BW, BH>, &inv_group_batch<BW, BH>});
 
 }  // namespace fft3d

@@ -25,6 +25,8 @@ struct SizeEntry {
   cudaError_t (*fwd_frames)(const ForwardArgs&, const FwdFrameSet&, int bytes_per_sample, cudaStream_t);
   // a run of frames filtered and inverse-transformed with one CTA per block
   cudaError_t (*inv_group)(const InverseArgs&, const TemporalSet&, int mode, cudaStream_t);
+  // and its batched form over the runs of many planes
+  cudaError_t (*inv_group_batch)(const BatchLaunch&, int mode, cudaStream_t);
 };
 
 bool register_size(const SizeEntry& e);

@@ -244,7 +244,8 @@ class Batch:
         out = (ctypes.c_double * 8)()
         _check(lib().fft3d_batch_stats(self.h, out))
         return dict(steps=int(out[0]), graph_launches=int(out[1]), tuning_steps=int(out[2]),
-                    kernels_last_step=int(out[4]), step_shapes=int(out[5]), wave_budget_mib=int(out[6]))
+                    kernels_last_step=int(out[4]), step_shapes=int(out[5]), wave_budget_mib=int(out[6]),
+                    host_ms_planning=out[3], host_ms_steps=out[7])
 
     def close(self):
         if getattr(self, "h", None):

@@ -220,3 +220,46 @@ def test_batch_timing_counts_phases(gpu):
     b.close()
     for e in engs:
         e.close()
+
+
+@pytest.mark.gpu
+def test_frame_groups_planes_larger_than_a_wave(gpu):
+    """A 1080p plane's new spectra and time-domain blocks (about 70 MB) exceed
+    the tuner's smallest wave budget (24 MiB), which its first step of every
+    shape tries: all frames of a plane's group, whose filter/inverse runs as
+    one run, must stay in one wave with the forward transforms it reads."""
+    import torch
+    Fb = 12
+    planes = synth.make_clip(1920, 1080, Fb, noise_sigma=5.0, seed=66)
+    p = make_params(sigma=2.5, bt=3, bw=32, bh=32, ow=16, oh=16, sharpen=0.2)
+    descs = plane_descs([a.shape[1:] for a in planes], 8, Fb)
+    dev = [torch.from_numpy(a).cuda() for a in planes]
+    ref = []
+    for a, d in zip(dev, descs):
+        e = engine.PlaneEngine(p, d)
+        o = torch.empty_like(a)
+        fb = a.shape[1] * a.shape[2]
+        for n in range(Fb):
+            ptrs, st = _window(a, n, Fb)
+            e.filter_device(n, ptrs, st, o.data_ptr() + n * fb, a.shape[2], 0)
+        torch.cuda.synchronize()
+        e.close()
+        ref.append(o.cpu().numpy())
+    engs = [engine.PlaneEngine(p, d) for d in descs]
+    outs = [torch.empty_like(a) for a in dev]
+    b = engine.Batch(tuning=True)
+    stream = torch.cuda.current_stream().cuda_stream
+    for n0 in range(0, Fb, 4):
+        items = []
+        for e, a, o in zip(engs, dev, outs):
+            fb = a.shape[1] * a.shape[2]
+            for n in range(n0, n0 + 4):
+                ptrs, st = _window(a, n, Fb)
+                items.append((e, n, ptrs, st, o.data_ptr() + n * fb, a.shape[2]))
+        b.step(items, stream)
+    torch.cuda.synchronize()
+    b.close()
+    for e in engs:
+        e.close()
+    for i, (r, o) in enumerate(zip(ref, outs)):
+        assert np.array_equal(r, o.cpu().numpy()), i
