@@ -439,6 +439,7 @@ fft3d::ForwardArgs forward_args(fft3d_plane* P, const void* plane, long long str
   a.wan_y = P->d_wan_y;
   for (int x = 0; x < fft3d::kMaxBw; x++) a.wx[x] = x < (int)P->h_wan_x.size() ? P->h_wan_x[x] : 0.f;
   a.spec = spec;
+  a.err = P->d_err;
   return a;
 }
 
@@ -592,6 +593,7 @@ int output_frame(fft3d_plane* P, float* tdom, const fft3d::Tables& tab, float ba
   oa.base = base;
   // float samples clamp to [0, 1] and have no integer maximum (no shift by 32)
   oa.maxval = P->bytes == 1 ? 255 : (P->bytes == 2 ? (1 << P->d.bits) - 1 : 0);
+  oa.err = P->d_err;
   if (g_defer) {
     g_defer->ola.push_back({oa, P->bytes, g_defer->plane});
   } else {
@@ -1173,8 +1175,9 @@ int finish_call(fft3d_plane* P, cudaEvent_t done, fft3d_plane::Stage* sg, bool l
     if (!flag) continue;
     int* dflag = k == 0 ? P->d_err : (learned ? fft3d::psd::err_flag(P->psd_model) : nullptr);
     if (dflag) cudaMemset(dflag, 0, sizeof(int));
-    return fail(FFT3D_E_CUDA, (flag & 2) ? "neo_fft3d: bulk copy completion wait timed out"
-                                         : "neo_fft3d: tensor-core MMA completion wait timed out");
+    return fail(FFT3D_E_CUDA, (flag & 4) ? "neo_fft3d: a bounds check of the checked build failed"
+                              : (flag & 2) ? "neo_fft3d: bulk copy completion wait timed out"
+                                           : "neo_fft3d: tensor-core MMA completion wait timed out");
   }
   return FFT3D_OK;
 }
@@ -1468,8 +1471,10 @@ int filter_group_host(fft3d_plane* P, int n0, int count, const void* const* src,
   give_sync_event(P, done);
   if (e != cudaSuccess) return cuda_fail(e, "synchronize");
   if (gs->h_flags[0]) {
+    const int flag = gs->h_flags[0];
     cudaMemset(P->d_err, 0, sizeof(int));
-    return fail(FFT3D_E_CUDA, "neo_fft3d: a bounded completion wait timed out");
+    return fail(FFT3D_E_CUDA, (flag & 4) ? "neo_fft3d: a bounds check of the checked build failed"
+                                         : "neo_fft3d: a bounded completion wait timed out");
   }
   return FFT3D_OK;
 }
@@ -1936,8 +1941,9 @@ int fft3d_plane_synchronize(fft3d_plane* P) {
   for (int k = 0; k < 2; k++) {
     if (!flags[k]) continue;
     CK(cudaMemset(k == 0 ? P->d_err : fft3d::psd::err_flag(P->psd_model), 0, sizeof(int)), "error flag");
-    return fail(FFT3D_E_CUDA, (flags[k] & 2) ? "neo_fft3d: bulk copy completion wait timed out"
-                                             : "neo_fft3d: tensor-core MMA completion wait timed out");
+    return fail(FFT3D_E_CUDA, (flags[k] & 4) ? "neo_fft3d: a bounds check of the checked build failed"
+                              : (flags[k] & 2) ? "neo_fft3d: bulk copy completion wait timed out"
+                                               : "neo_fft3d: tensor-core MMA completion wait timed out");
   }
   return FFT3D_OK;
 }

@@ -68,6 +68,9 @@ __device__ __forceinline__ void overlap_add_px(const OlaArgs& a, int x0, int k) 
   const bool yov = y < g.oh, xov = x < g.ow;
   const int bw = g.bw, bh = g.bh;
   auto at = [&](int bxx, int byy, int yy, int xx) {
+    if (!FFT3D_IN(bxx >= 0 && bxx < g.nox && byy >= 0 && byy < g.noy && yy >= 0 && yy < bh && xx >= 0 && xx < bw,
+                  a.err))
+      return 0.f;
     return __ldg(a.tdom + ((size_t)(byy * g.nox + bxx) * bh + yy) * bw + xx);
   };
   const float norm = a.norm;
@@ -89,7 +92,9 @@ __device__ __forceinline__ void overlap_add_px(const OlaArgs& a, int x0, int k) 
       v = ((aa * sxr + b * sxl) * wr + (c * sxr + d * sxl) * wl) + a.rounder + a.base;
     }
   }
-  T* row = reinterpret_cast<T*>(static_cast<char*>(a.dst) + (long long)field_row(k, g.H, g.interlaced) * a.dst_stride);
+  const int fr = field_row(k, g.H, g.interlaced);
+  if (!FFT3D_IN(fr >= 0 && fr < g.H, a.err)) return;
+  T* row = reinterpret_cast<T*>(static_cast<char*>(a.dst) + (long long)fr * a.dst_stride);
   store_sample<T>(row + x0, v, a.maxval);
 }
 
@@ -138,8 +143,12 @@ __device__ __forceinline__ void overlap_add_px4(const OlaArgs& a, int x0, int k)
   // time-domain values are read once: not kept in L1, where the synthesis
   // windows stay
   auto at4 = [&](int bxx, int byy, int yy, int xx) {
+    float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (!FFT3D_IN(bxx >= 0 && bxx < g.nox && byy >= 0 && byy < g.noy && yy >= 0 && yy < bh && xx >= 0 &&
+                      xx + 3 < bw,
+                  a.err))
+      return q;
     const float* p = a.tdom + ((size_t)(byy * g.nox + bxx) * bh + yy) * bw + xx;
-    float4 q;
     asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
         : "=f"(q.x), "=f"(q.y), "=f"(q.z), "=f"(q.w)
         : "l"(p));
@@ -176,7 +185,9 @@ __device__ __forceinline__ void overlap_add_px4(const OlaArgs& a, int x0, int k)
       }
     }
   }
-  T* row = reinterpret_cast<T*>(static_cast<char*>(a.dst) + (long long)field_row(k, g.H, g.interlaced) * a.dst_stride);
+  const int fr = field_row(k, g.H, g.interlaced);
+  if (!FFT3D_IN(fr >= 0 && fr < g.H && x0 + 3 < g.W, a.err)) return;
+  T* row = reinterpret_cast<T*>(static_cast<char*>(a.dst) + (long long)fr * a.dst_stride);
   typename Pack4<T>::V o;
   o.x = clamp_sample<T>(v[0], a.maxval);
   o.y = clamp_sample<T>(v[1], a.maxval);

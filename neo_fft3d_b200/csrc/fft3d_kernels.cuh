@@ -64,6 +64,24 @@ struct FilterConsts {
   int use_sharpen, use_dehalo;
 };
 
+// Bounds-checked build (the kernels compiled with -DFFT3D_CHECKED=1, into
+// lib/libfft3d_b200_checked.so): FFT3D_IN(cond, err) is `cond`, and when it is
+// false the access it guards is skipped and bit 2 of the device error flag is
+// set, which the host-buffer calls and fft3d_plane_synchronize report. In the
+// regular build it is `true` (the condition is not even evaluated).
+#ifndef FFT3D_CHECKED
+#define FFT3D_CHECKED 0
+#endif
+__device__ __forceinline__ bool checked_in(bool ok, int* err) {
+  if (!ok && err) atomicOr(err, 4);
+  return ok;
+}
+#if FFT3D_CHECKED
+#define FFT3D_IN(cond, err) ::fft3d::checked_in((cond), (err))
+#else
+#define FFT3D_IN(cond, err) true
+#endif
+
 constexpr int kMaxBw = 64;  // largest block width the kernels are built for (48) rounded up
 struct ForwardArgs {
   Geom g;
@@ -73,6 +91,7 @@ struct ForwardArgs {
   const float* wan_x;
   const float* wan_y;
   float2* spec;           // blocks x bh x nh
+  int* err;               // device error flag (bounds-checked build), or null
   float wx[kMaxBw];       // wan_x by value: read through the launch parameters
                           // (constant-bank operands) by the per-plane kernels
 };
@@ -90,7 +109,8 @@ struct InverseArgs {
                           // [blocks][bh*nh] when psd_per_block, else [bh*nh]
   float psd_scale;        // btcur for Wiener 3D (pattern3d = bt x pattern2d), else 1
   int psd_per_block;
-  int* err;               // device error flag (bit 1: a bounded bulk-copy wait ran out)
+  int* err;               // device error flag (bit 0: a bounded tensor-core wait ran out, bit 1: a
+                          // bounded bulk-copy wait, bit 2: a bounds check of the checked build)
   int bulk;               // use the bulk-staged filter/inverse kernel where it applies
   int reverse;            // walk the blocks from the end (alternated per frame so
                           // that the blocks read last stay in L2 for the next frame)
@@ -174,6 +194,7 @@ struct OlaArgs {
   float rounder;          // 0.5 for integer formats, 0 for float
   float base;
   int maxval;             // (1 << bits) - 1
+  int* err;               // device error flag (bounds-checked build), or null
 };
 
 // One batched launch: `nitems` work items (plane index into `args`, CTA of

@@ -108,15 +108,18 @@ struct FrameFwd {
   __device__ __forceinline__ float2* spec() const { return sp; }
 };
 
-// Source row of row y of block `blk` and the source column of its column 0.
+// Source row of row y of block `blk` and the source column of its column 0;
+// *row: the source row index (checked against the plane in the checked build).
 template <typename T, class Win>
-__device__ __forceinline__ const T* fwd_row_src(const ForwardArgs& a, const Win& win, int blk, int y, int* x0) {
+__device__ __forceinline__ const T* fwd_row_src(const ForwardArgs& a, const Win& win, int blk, int y, int* x0,
+                                                int* row = nullptr) {
   const Geom& g = a.g;
   const int by = blk / g.nox, bx = blk - by * g.nox;
   const int k = reflect101(by * g.sy + y - g.sy, g.H);
   *x0 = bx * g.sx - g.sx;
-  return reinterpret_cast<const T*>(static_cast<const char*>(win.src()) +
-                                    (long long)field_row(k, g.H, g.interlaced) * win.stride());
+  const int r = field_row(k, g.H, g.interlaced);
+  if (row) *row = r;
+  return reinterpret_cast<const T*>(static_cast<const char*>(win.src()) + (long long)r * win.stride());
 }
 
 // Rows whose BW samples are whole 16-byte vectors (8- and 16-bit samples) can
@@ -157,19 +160,23 @@ __device__ __forceinline__ void fwd_row(const ForwardArgs& a, const Win& win, in
                                         const uint4* raw) {
   constexpr int NH = BW / 2 + 1;
   const Geom& g = a.g;
-  int x0;
-  const T* srow = fwd_row_src<T>(a, win, blk, y, &x0);
+  int x0, srcrow;
+  const T* srow = fwd_row_src<T>(a, win, blk, y, &x0, &srcrow);
   float r[BW];
   if constexpr (raw_vectors<BW, T>() > 0) {
     if (raw) decode_row<BW, T>(raw, a.base, r);  // already minus base
   }
   if (raw_vectors<BW, T>() > 0 && raw) {
   } else {
+    const bool row_ok = FFT3D_IN(srcrow >= 0 && srcrow < g.H, a.err);
     if (x0 >= 0 && x0 + BW <= g.W) {
-      load_row<T, BW>(srow + x0, r);
+      if (row_ok) load_row<T, BW>(srow + x0, r);
     } else {
 #pragma unroll
-      for (int x = 0; x < BW; x++) r[x] = load_sample<T>(srow + reflect101(x0 + x, g.W));
+      for (int x = 0; x < BW; x++) {
+        const int xi = reflect101(x0 + x, g.W);
+        r[x] = (row_ok && FFT3D_IN(xi >= 0 && xi < g.W, a.err)) ? load_sample<T>(srow + xi) : 0.f;
+      }
     }
 #pragma unroll
     for (int x = 0; x < BW; x++) r[x] = r[x] - a.base;
@@ -301,10 +308,11 @@ __device__ __forceinline__ void forward_cta_w(const ForwardArgs& a, int cta, con
       const int t = lane + 32 * i, b = t / BH, y = t - b * BH;
       have[i] = false;
       if (t < NBW * BH && blk0 + b < g.nblocks) {
-        int x0;
-        const T* srow = fwd_row_src<T>(a, win, blk0 + b, y, &x0);
+        int x0, row;
+        const T* srow = fwd_row_src<T>(a, win, blk0 + b, y, &x0, &row);
         const T* p = srow + x0;
-        if (x0 >= 0 && x0 + BW <= g.W && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+        if (x0 >= 0 && x0 + BW <= g.W && (reinterpret_cast<uintptr_t>(p) & 15) == 0 &&
+            FFT3D_IN(row >= 0 && row < g.H, a.err)) {
 #pragma unroll
           for (int v = 0; v < NV; v++) raw[i][v] = __ldg(reinterpret_cast<const uint4*>(p) + v);
           have[i] = true;
@@ -332,7 +340,9 @@ __device__ __forceinline__ void forward_cta_w(const ForwardArgs& a, int cta, con
   const int nvalid = min(NBW, g.nblocks - blk0);
   float4* dst = reinterpret_cast<float4*>(win.spec() + (size_t)blk0 * BINS);
   const float4* src = reinterpret_cast<const float4*>(S);
-  for (int i = lane; i < nvalid * BINS / 2; i += 32) dst[i] = src[i];
+  for (int i = lane; i < nvalid * BINS / 2; i += 32)
+    if (FFT3D_IN((size_t)blk0 * BINS / 2 + i < (size_t)g.nblocks * BINS / 2 && win.spec() != nullptr, a.err))
+      dst[i] = src[i];
   __syncwarp();  // S is reused by the warp's next work item
 }
 
@@ -799,7 +809,10 @@ __device__ __forceinline__ void filter_inverse_cta_w(const InverseArgs& a, int v
     auto load = [&](int j, float2(&dst)[NGB]) {
       const int i = lane + 32 * j;
 #pragma unroll
-      for (int k = 0; k < NG; k++) dst[k] = i < BINS ? ld_stream(win.in(LO + k) + off + i) : make_float2(0.f, 0.f);
+      for (int k = 0; k < NG; k++)
+        dst[k] = (i < BINS && FFT3D_IN(win.in(LO + k) != nullptr && off + i < (size_t)g.nblocks * BINS, a.err))
+                     ? ld_stream(win.in(LO + k) + off + i)
+                     : make_float2(0.f, 0.f);
     };
     if constexpr (NG > 0) {
 #pragma unroll
@@ -849,7 +862,7 @@ __device__ __forceinline__ void filter_inverse_cta_w(const InverseArgs& a, int v
   }
   __syncwarp();
   for (int b = 0; b < NBW && blk0 + b < g.nblocks; b++)
-    store_tdom<BW, BH>(S + b * BINS, win.tdom() + (size_t)(blk0 + b) * BH * BW, lane);
+    if (FFT3D_IN(win.tdom() != nullptr, a.err)) store_tdom<BW, BH>(S + b * BINS, win.tdom() + (size_t)(blk0 + b) * BH * BW, lane);
   __syncwarp();  // S is reused by the warp's next work item
 }
 
@@ -939,6 +952,16 @@ __host__ __device__ constexpr int group_smem_bytes(int count) {
 // Every bin and every transform uses the arithmetic of k_filter_inverse
 // (filter_vals, kalman_step, sharpen_bin, inv_col, inv_row_inplace), so the
 // output equals one frame per launch.
+// A run's window spectrum s, bins bin and bin + 1 of the block at `off`
+// (checked build: the spectrum exists and the pair lies in the plane).
+__device__ __forceinline__ float4 group_load(const InverseArgs& a, const TemporalSet& ts, int s, size_t off, int bin) {
+  if (!FFT3D_IN(s >= 0 && s < kGroupTile + 4 && ts.spec[s] != nullptr &&
+                    off + bin + 1 < (size_t)a.g.nblocks * a.g.bh * a.g.nh,
+                a.err))
+    return make_float4(0.f, 0.f, 0.f, 0.f);
+  return ld_stream4(ts.spec[s] + off + bin);
+}
+
 template <int MODE>
 __device__ __forceinline__ void group_filter_pair(const InverseArgs& a, const TemporalSet& ts, size_t off, int bin,
                                                   int count, const float* gfs, float* gsh, float gs0, float2* tile,
@@ -961,10 +984,10 @@ __device__ __forceinline__ void group_filter_pair(const InverseArgs& a, const Te
       s0 = fmaxf(__ldg(a.t.pattern2d + bin), 1e-15f);
       s1 = fmaxf(__ldg(a.t.pattern2d + bin + 1), 1e-15f);
     }
-    float4 nxt = ld_stream4(ts.spec[2] + off + bin);
+    float4 nxt = group_load(a, ts, 2, off, bin);
     for (int j = 0; j < count; j++) {
       const float4 c = nxt;
-      if (j + 1 < count) nxt = ld_stream4(ts.spec[j + 3] + off + bin);
+      if (j + 1 < count) nxt = group_load(a, ts, j + 3, off, bin);
       kalman_step(a, make_float2(c.x, c.y), s0, l0, cv.x, cp.x);
       kalman_step(a, make_float2(c.z, c.w), s1, l1, cv.y, cp.y);
       out(j, l0, l1);
@@ -974,7 +997,7 @@ __device__ __forceinline__ void group_filter_pair(const InverseArgs& a, const Te
     *reinterpret_cast<float2*>(a.kal_covarp + off + bin) = cp;
   } else if constexpr (MODE == MODE_SHARPEN_ONLY) {
     for (int j = 0; j < count; j++) {
-      const float4 c = ld_stream4(ts.spec[j + 2] + off + bin);
+      const float4 c = group_load(a, ts, j + 2, off, bin);
       out(j, make_float2(c.x, c.y), make_float2(c.z, c.w));
     }
   } else {
@@ -984,15 +1007,15 @@ __device__ __forceinline__ void group_filter_pair(const InverseArgs& a, const Te
     // index below is a compile-time constant
     float4 r[NW];
 #pragma unroll
-    for (int k = 0; k < NW - 1; k++) r[(LO + k) % NW] = ld_stream4(ts.spec[LO + k] + off + bin);
-    float4 nxt = ld_stream4(ts.spec[HI] + off + bin);
+    for (int k = 0; k < NW - 1; k++) r[(LO + k) % NW] = group_load(a, ts, LO + k, off, bin);
+    float4 nxt = group_load(a, ts, HI, off, bin);
     for (int j0 = 0; j0 < count; j0 += NW) {
 #pragma unroll
       for (int u = 0; u < NW; u++) {
         const int j = j0 + u;
         if (j < count) {
           r[(u + HI) % NW] = nxt;
-          if (j + 1 < count) nxt = ld_stream4(ts.spec[j + 1 + HI] + off + bin);
+          if (j + 1 < count) nxt = group_load(a, ts, j + 1 + HI, off, bin);
           float2 w0[5], w1[5];
 #pragma unroll
           for (int k = 0; k < 5; k++) {
@@ -1017,7 +1040,7 @@ __device__ __forceinline__ void group_filter_one(const InverseArgs& a, const Tem
   constexpr int LO = win_lo<MODE>(), HI = win_hi<MODE>();
   float4 r[5];
 #pragma unroll
-  for (int k = LO; k <= HI; k++) r[k] = ld_stream4(ts.spec[j + k] + off + bin);
+  for (int k = LO; k <= HI; k++) r[k] = group_load(a, ts, j + k, off, bin);
   float2 w0[5], w1[5];
 #pragma unroll
   for (int k = 0; k < 5; k++) {
@@ -1050,7 +1073,9 @@ __device__ __forceinline__ void filter_inverse_group_cta(const InverseArgs& a, c
   const float gs0 = __ldg(&a.t.grid[0].x);
   const int t = threadIdx.x;
   // 0. grid fraction of each frame's block (its DC)
-  if (MODE >= 1 && t < count) gfs[t] = a.c.degrid * __ldg(&ts.spec[t + 2][off].x) / gs0;
+  if (MODE >= 1 && t < count)
+    gfs[t] = FFT3D_IN(ts.spec[t + 2] != nullptr && blk < a.g.nblocks, a.err)
+                 ? a.c.degrid * __ldg(&ts.spec[t + 2][off].x) / gs0 : 0.f;
   __syncthreads();
   // 1. filter: whole rounds of bin pairs over all frames; the remaining pairs
   //    (a partial round) as (pair, frame) items spread over every thread,
@@ -1115,7 +1140,8 @@ __device__ __forceinline__ void filter_inverse_group_cta(const InverseArgs& a, c
   for (int i = t; i < count * BH * HALF; i += NT) {
     const int j = i / (BH * HALF), r = i - j * (BH * HALF);
     const int y = r / HALF, x = r - y * HALF;
-    reinterpret_cast<float2*>(ts.tdom[j] + (size_t)blk * BH * BW)[r] = S[j * BINS + y * NH + x];
+    if (FFT3D_IN(ts.tdom[j] != nullptr && blk < a.g.nblocks, a.err))
+      reinterpret_cast<float2*>(ts.tdom[j] + (size_t)blk * BH * BW)[r] = S[j * BINS + y * NH + x];
   }
 }
 

@@ -252,6 +252,7 @@ extern "C" int fft3d_filter2d_static(const fft3d_params* p0, const fft3d_plane_d
   fa.wan_x = tab.wan_x;
   fa.wan_y = tab.wan_y;
   fa.spec = spec;
+  fa.err = nullptr;
   for (int x = 0; x < fft3d::kMaxBw; x++) fa.wx[x] = x < ep.bw ? blob[o_wx + x] : 0.f;
   err = fft3d::launch_forward(fa, bytes, st);
   if (err != cudaSuccess) return sfail(FFT3D_E_CUDA, std::string("neo_fft3d: forward kernel: ") + cudaGetErrorString(err));
@@ -297,6 +298,7 @@ extern "C" int fft3d_filter2d_static(const fft3d_params* p0, const fft3d_plane_d
   oa.rounder = ints ? 0.5f : 0.f;
   oa.base = base_val;
   oa.maxval = bytes == 1 ? 255 : (bytes == 2 ? (1 << d->bits) - 1 : 0);  // float: clamp to [0, 1]
+  oa.err = nullptr;
   err = fft3d::launch_overlap_add(oa, bytes, st);
   if (err != cudaSuccess) return sfail(FFT3D_E_CUDA, std::string("neo_fft3d: overlap-add kernel: ") + cudaGetErrorString(err));
   return FFT3D_OK;
