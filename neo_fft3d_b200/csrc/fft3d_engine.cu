@@ -102,6 +102,14 @@ struct fft3d_plane {
   // launch for the run, then a sharpen/inverse launch; 0 (=fused): one
   // filter/inverse launch per Wiener 3D run, frames interleaved by CTA
   int group_split = 2;
+  // NEO_FFT3D_FUSED_OLA=1: a run's overlap-adds are done by its
+  // filter/inverse launch instead of a separate overlap-add launch (measured
+  // slower: the tile overlap-adds at the CTAs' tails are latency-bound);
+  // per-tile arrival counters (nox x noy, zeroed once) and the launch epoch
+  // their targets count in
+  unsigned* d_ola_cnt = nullptr;
+  unsigned ola_epoch = 0;
+  bool fuse_ola = false;
   int occ = 0;
   int keep_lo = 1, keep_hi = 0;
   int fixed_reverse = -1;
@@ -364,6 +372,7 @@ void free_plane(fft3d_plane* P) {
   cudaFree(P->d_pshow_win);
   for (auto* t : P->tdom_extra) cudaFree(t);
   for (auto* f : P->filt_frames) cudaFree(f);
+  cudaFree(P->d_ola_cnt);
   cudaFree(P->d_filt);
   cudaFree(P->d_tc);
   cudaFree(P->d_err);
@@ -1005,11 +1014,75 @@ void discard_recorded(fft3d_plane* P, const fft3d::Deferred& d) {
       if (s.spec == f.a.spec) s.frame = -1;
 }
 
+// Fuses the overlap-adds of the run d.inv[i, e) into its filter/inverse
+// launch (fills *of, marks the records in ola_done) when the plane asks for
+// it (NEO_FFT3D_FUSED_OLA=1) and allows it:
+// every frame of the run has its overlap-add record, and the plane's output
+// tiles are inside its block grid. Otherwise (or when the arrival counters
+// cannot be allocated) the overlap-adds stay separate launches.
+bool fuse_run_ola(fft3d_plane* P, const fft3d::Deferred& d, const fft3d::TemporalSet& ts, size_t i, size_t e,
+                  std::vector<char>& ola_done, fft3d::OlaFuse* of, cudaStream_t st) {
+  if (!P->fuse_ola || e - i > (size_t)fft3d::kGroupTile) return false;
+  const fft3d::Geom& g = P->g;
+  const int tiles_x = (g.sx + g.W - 1) / g.sx, tiles_y = (g.sy + g.H - 1) / g.sy;
+  if (tiles_x < 1 || tiles_y < 1 || tiles_x >= g.nox || tiles_y >= g.noy) return false;
+  size_t idx[fft3d::kGroupTile];
+  for (size_t k = i; k < e; k++) {
+    size_t m = 0;
+    while (m < d.ola.size() && (ola_done[m] || d.ola[m].a.tdom != d.inv[k].a.tdom)) m++;
+    if (m == d.ola.size() || (k > i && d.ola[m].bytes != d.ola[idx[0]].bytes)) return false;
+    idx[k - i] = m;
+  }
+  const size_t cnt_bytes = (size_t)g.nblocks * sizeof(unsigned);
+  if (!P->d_ola_cnt) {
+    if (dmalloc(P, &P->d_ola_cnt, cnt_bytes) != cudaSuccess) {
+      cudaGetLastError();
+      P->d_ola_cnt = nullptr;
+      return false;
+    }
+    if (cudaMemsetAsync(P->d_ola_cnt, 0, cnt_bytes, st) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFree(P->d_ola_cnt);
+      P->d_ola_cnt = nullptr;
+      return false;
+    }
+    P->ola_epoch = 0;
+  }
+  if (P->ola_epoch >= (1u << 29)) {  // targets stay below 2^32: start the counts over
+    if (cudaMemsetAsync(P->d_ola_cnt, 0, cnt_bytes, st) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    P->ola_epoch = 0;
+  }
+  P->ola_epoch++;
+  *of = fft3d::OlaFuse{};
+  of->o = d.ola[idx[0]].a;
+  of->o.tdom = nullptr;
+  of->o.dst = nullptr;
+  fft3d::OlaFrameSet fs{};
+  fs.count = (int)(e - i);
+  for (size_t k = 0; k < e - i; k++) {
+    of->dst[k] = d.ola[idx[k]].a.dst;
+    of->dst_stride[k] = d.ola[idx[k]].a.dst_stride;
+    fs.tdom[k] = ts.tdom[k];
+    fs.dst[k] = of->dst[k];
+    fs.dst_stride[k] = of->dst_stride[k];
+    ola_done[idx[k]] = 1;
+  }
+  of->cnt = P->d_ola_cnt;
+  of->epoch = P->ola_epoch;
+  of->tiles_x = tiles_x;
+  of->tiles_y = tiles_y;
+  of->bytes = d.ola[idx[0]].bytes;
+  of->px4 = fft3d::overlap_add_frames_supported(of->o, fs, of->bytes) ? 1 : 0;
+  return true;
+}
+
 // Issues the launches of a frame group recorded for plane P, phase by phase:
-// the new spectra, then the filter/inverse of runs of consecutive frames of
-// one Wiener 3D mode as one k_filter_inverse_frames launch each (the other
-// frames, e.g. the clip-edge ones, one launch each), the crop-border copies
-// and the overlap-adds.
+// the new spectra, the plane copies (crop borders), then the filter/inverse
+// of runs of consecutive frames of one mode (with their overlap-adds when
+// fused), then the remaining overlap-adds.
 int run_group(fft3d_plane* P, const fft3d::Deferred& d, cudaStream_t st) {
   const double S = (double)P->spec_elems() * sizeof(float2);
   const double T = (double)P->g.nblocks * P->g.bh * P->g.bw * 4;
@@ -1036,6 +1109,13 @@ int run_group(fft3d_plane* P, const fft3d::Deferred& d, cudaStream_t st) {
     g_launches++;
     i = e;
   }
+  // the plane copies (a cropped frame's source plane, whose interior the
+  // overlap-add then overwrites; Kalman frame 0): before any overlap-add,
+  // which a run's filter/inverse launch may do itself
+  for (const auto& c : d.copies)
+    CK(cudaMemcpy2DAsync(c.dst, c.dpitch, c.src, c.spitch, c.width, c.height, cudaMemcpyDeviceToDevice, st),
+       "plane copy");
+  std::vector<char> ola_done(d.ola.size(), 0);  // overlap-adds done by a run's launch
   for (size_t i = 0; P->group_split == 2 && i < d.inv.size();) {
     // One launch per run of up to kGroupTile consecutive frames of one mode,
     // one CTA per block: each window spectrum (and a Kalman state) is read
@@ -1057,11 +1137,16 @@ int run_group(fft3d_plane* P, const fft3d::Deferred& d, cudaStream_t st) {
       ts.tdom[k - i] = d.inv[k].a.tdom;
     }
     const double state = mode == fft3d::MODE_KALMAN ? 2.0 * (double)P->spec_elems() * 16 : 0.0;
-    // reads: each window spectrum of the run once (+ Kalman state); writes: the time-domain blocks
-    TimeScope tsc(P, K_INVERSE, (double)seen.size() * S + state + n * T, st);
+    fft3d::OlaFuse of{};
+    const bool fused = fuse_run_ola(P, d, ts, i, e, ola_done, &of, st);
+    // reads: each window spectrum of the run once (+ Kalman state); writes: the
+    // time-domain blocks, or with the overlap-adds fused the output pixels
+    TimeScope tsc(P, K_INVERSE, (double)seen.size() * S + state + n * (fused ? pix : T), st);
     fft3d::InverseArgs ga = d.inv[i].a;
     for (auto& p : ga.in) p = nullptr;
-    CK(fft3d::launch_filter_inverse_group(ga, ts, mode, st), "filter/inverse kernel (frame group)");
+    const cudaError_t le = fft3d::launch_filter_inverse_group(ga, ts, mode, st, fused ? &of : nullptr);
+    if (le != cudaSuccess && fused) P->ola_epoch--;  // no arrivals were counted for this epoch
+    CK(le, "filter/inverse kernel (frame group)");
     g_launches++;
     i = e;
   }
@@ -1136,30 +1221,30 @@ int run_group(fft3d_plane* P, const fft3d::Deferred& d, cudaStream_t st) {
     g_launches++;
     i = e;
   }
-  for (const auto& c : d.copies)
-    CK(cudaMemcpy2DAsync(c.dst, c.dpitch, c.src, c.spitch, c.width, c.height, cudaMemcpyDeviceToDevice, st),
-       "plane copy");
-  // the overlap-adds: one launch for all frames where the 4-pixel kernel applies
+  // the other overlap-adds: one launch for all frames where the 4-pixel kernel applies
+  std::vector<const fft3d::Deferred::Ola*> rest;
+  for (size_t k = 0; k < d.ola.size(); k++)
+    if (!ola_done[k]) rest.push_back(&d.ola[k]);
   bool merged = false;
-  if (d.ola.size() > 1 && d.ola.size() <= (size_t)fft3d::kMaxGroupFrames) {
+  if (rest.size() > 1 && rest.size() <= (size_t)fft3d::kMaxGroupFrames) {
     fft3d::OlaFrameSet fs{};
-    fs.count = (int)d.ola.size();
-    for (size_t k = 0; k < d.ola.size(); k++) {
-      fs.tdom[k] = d.ola[k].a.tdom;
-      fs.dst[k] = d.ola[k].a.dst;
-      fs.dst_stride[k] = d.ola[k].a.dst_stride;
+    fs.count = (int)rest.size();
+    for (size_t k = 0; k < rest.size(); k++) {
+      fs.tdom[k] = rest[k]->a.tdom;
+      fs.dst[k] = rest[k]->a.dst;
+      fs.dst_stride[k] = rest[k]->a.dst_stride;
     }
-    if (fft3d::overlap_add_frames_supported(d.ola[0].a, fs, d.ola[0].bytes)) {
-      TimeScope ts(P, K_OLA, (double)d.ola.size() * (T + pix), st);
-      CK(fft3d::launch_overlap_add_frames(d.ola[0].a, fs, d.ola[0].bytes, st), "overlap-add kernel (frame group)");
+    if (fft3d::overlap_add_frames_supported(rest[0]->a, fs, rest[0]->bytes)) {
+      TimeScope ts(P, K_OLA, (double)rest.size() * (T + pix), st);
+      CK(fft3d::launch_overlap_add_frames(rest[0]->a, fs, rest[0]->bytes, st), "overlap-add kernel (frame group)");
       merged = true;
       g_launches++;
     }
   }
   if (!merged)
-    for (const auto& o : d.ola) {
+    for (const auto* o : rest) {
       TimeScope ts(P, K_OLA, T + pix, st);
-      CK(fft3d::launch_overlap_add(o.a, o.bytes, st), "overlap-add kernel");
+      CK(fft3d::launch_overlap_add(o->a, o->bytes, st), "overlap-add kernel");
       g_launches++;
     }
   return FFT3D_OK;
@@ -1522,6 +1607,8 @@ int fft3d_plane_create(const fft3d_params* p, const fft3d_plane_desc* d, int dev
     const char* gf = std::getenv("NEO_FFT3D_GROUP_FILTER");
     const std::string gv = gf ? gf : "block";
     P->group_split = gv == "fused" ? 0 : (gv == "split" ? 1 : 2);
+    const char* fo = std::getenv("NEO_FFT3D_FUSED_OLA");
+    P->fuse_ola = fo && std::string(fo) == "1";
   }
   fft3d_params& ep = P->ep;
   if (d->bits < 8 || (d->bits > 16 && d->bits != 32)) { delete P; return fail(FFT3D_E_PARAM, "neo_fft3d: unsupported bit depth"); }

@@ -35,167 +35,6 @@ std::vector<SizeEntry>& table() {
   return t;
 }
 
-template <typename T>
-__device__ __forceinline__ void store_sample(T* p, float v, int maxval);
-template <>
-__device__ __forceinline__ void store_sample<uint8_t>(uint8_t* p, float v, int maxval) {
-  int i = __float2int_rz(v);  // C cast: truncation toward zero (src/buffer.cpp:406)
-  i = i < 0 ? 0 : (i > maxval ? maxval : i);
-  *p = (uint8_t)i;
-}
-template <>
-__device__ __forceinline__ void store_sample<uint16_t>(uint16_t* p, float v, int maxval) {
-  int i = __float2int_rz(v);
-  i = i < 0 ? 0 : (i > maxval ? maxval : i);
-  *p = (uint16_t)i;
-}
-template <>
-__device__ __forceinline__ void store_sample<float>(float* p, float v, int) {
-  float c = v < 0.f ? 0.f : v;  // float samples clamp to [0, 1] (src/buffer.cpp:397)
-  *p = c > 1.f ? 1.f : c;
-}
-
-// One thread per output pixel of the processed region: the (at most four)
-// blocks covering it, weighted with the synthesis windows and the FFT
-// normalisation in the association order of src/buffer.cpp:399-559.
-template <typename T>
-__device__ __forceinline__ void overlap_add_px(const OlaArgs& a, int x0, int k) {
-  const Geom& g = a.g;
-  if (x0 >= g.W || k >= g.H) return;
-  const int Y = g.sy + k, X = g.sx + x0;
-  const int by = Y / g.sy, y = Y - by * g.sy;
-  const int bx = X / g.sx, x = X - bx * g.sx;
-  const bool yov = y < g.oh, xov = x < g.ow;
-  const int bw = g.bw, bh = g.bh;
-  auto at = [&](int bxx, int byy, int yy, int xx) {
-    if (!FFT3D_IN(bxx >= 0 && bxx < g.nox && byy >= 0 && byy < g.noy && yy >= 0 && yy < bh && xx >= 0 && xx < bw,
-                  a.err))
-      return 0.f;
-    return __ldg(a.tdom + ((size_t)(byy * g.nox + bxx) * bh + yy) * bw + xx);
-  };
-  const float norm = a.norm;
-  float v;
-  if (!yov) {
-    const float d = at(bx, by, y, x);
-    if (!xov) v = d * norm + a.rounder + a.base;
-    else {
-      const float c = at(bx - 1, by, y, x + g.sx);
-      v = (c * __ldg(a.t.wsyn_xr + x) + d * __ldg(a.t.wsyn_xl + x)) * norm + a.rounder + a.base;
-    }
-  } else {
-    const float wr = __ldg(a.t.wsyn_yr + y) * norm, wl = __ldg(a.t.wsyn_yl + y) * norm;
-    const float b = at(bx, by - 1, y + g.sy, x), d = at(bx, by, y, x);
-    if (!xov) v = (b * wr + d * wl) + a.rounder + a.base;
-    else {
-      const float aa = at(bx - 1, by - 1, y + g.sy, x + g.sx), c = at(bx - 1, by, y, x + g.sx);
-      const float sxr = __ldg(a.t.wsyn_xr + x), sxl = __ldg(a.t.wsyn_xl + x);
-      v = ((aa * sxr + b * sxl) * wr + (c * sxr + d * sxl) * wl) + a.rounder + a.base;
-    }
-  }
-  const int fr = field_row(k, g.H, g.interlaced);
-  if (!FFT3D_IN(fr >= 0 && fr < g.H, a.err)) return;
-  T* row = reinterpret_cast<T*>(static_cast<char*>(a.dst) + (long long)fr * a.dst_stride);
-  store_sample<T>(row + x0, v, a.maxval);
-}
-
-// Four adjacent output pixels per thread (x0 a multiple of 4), for planes
-// whose block step, overlap, width and block width are multiples of 4 and
-// whose destination rows are aligned for a 4-sample store: the four pixels
-// share their blocks and overlap case, so the tdom reads are float4 loads,
-// the block indices are computed once and the samples go out in one store.
-// Each pixel's arithmetic is overlap_add_px's, term for term.
-template <typename T>
-struct Pack4;
-template <>
-struct Pack4<uint8_t> {
-  using V = uchar4;
-};
-template <>
-struct Pack4<uint16_t> {
-  using V = ushort4;
-};
-template <>
-struct Pack4<float> {
-  using V = float4;
-};
-
-template <typename T>
-__device__ __forceinline__ T clamp_sample(float v, int maxval) {
-  if constexpr (sizeof(T) == 4) {
-    float c = v < 0.f ? 0.f : v;
-    return c > 1.f ? 1.f : c;
-  } else {
-    int i = __float2int_rz(v);
-    i = i < 0 ? 0 : (i > maxval ? maxval : i);
-    return (T)i;
-  }
-}
-
-template <typename T>
-__device__ __forceinline__ void overlap_add_px4(const OlaArgs& a, int x0, int k) {
-  const Geom& g = a.g;
-  if (x0 >= g.W || k >= g.H) return;
-  const int Y = g.sy + k, X = g.sx + x0;
-  const int by = Y / g.sy, y = Y - by * g.sy;
-  const int bx = X / g.sx, x = X - bx * g.sx;
-  const bool yov = y < g.oh, xov = x < g.ow;
-  const int bw = g.bw, bh = g.bh;
-  // time-domain values are read once: not kept in L1, where the synthesis
-  // windows stay
-  auto at4 = [&](int bxx, int byy, int yy, int xx) {
-    float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (!FFT3D_IN(bxx >= 0 && bxx < g.nox && byy >= 0 && byy < g.noy && yy >= 0 && yy < bh && xx >= 0 &&
-                      xx + 3 < bw,
-                  a.err))
-      return q;
-    const float* p = a.tdom + ((size_t)(byy * g.nox + bxx) * bh + yy) * bw + xx;
-    asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
-        : "=f"(q.x), "=f"(q.y), "=f"(q.z), "=f"(q.w)
-        : "l"(p));
-    return q;
-  };
-  auto comp = [](const float4& q, int i) { return i == 0 ? q.x : (i == 1 ? q.y : (i == 2 ? q.z : q.w)); };
-  const float norm = a.norm;
-  float v[4];
-  if (!yov) {
-    const float4 d = at4(bx, by, y, x);
-    if (!xov) {
-#pragma unroll
-      for (int i = 0; i < 4; i++) v[i] = comp(d, i) * norm + a.rounder + a.base;
-    } else {
-      const float4 c = at4(bx - 1, by, y, x + g.sx);
-#pragma unroll
-      for (int i = 0; i < 4; i++)
-        v[i] = (comp(c, i) * __ldg(a.t.wsyn_xr + x + i) + comp(d, i) * __ldg(a.t.wsyn_xl + x + i)) * norm + a.rounder +
-               a.base;
-    }
-  } else {
-    const float wr = __ldg(a.t.wsyn_yr + y) * norm, wl = __ldg(a.t.wsyn_yl + y) * norm;
-    const float4 b = at4(bx, by - 1, y + g.sy, x), d = at4(bx, by, y, x);
-    if (!xov) {
-#pragma unroll
-      for (int i = 0; i < 4; i++) v[i] = (comp(b, i) * wr + comp(d, i) * wl) + a.rounder + a.base;
-    } else {
-      const float4 aa = at4(bx - 1, by - 1, y + g.sy, x + g.sx), c = at4(bx - 1, by, y, x + g.sx);
-#pragma unroll
-      for (int i = 0; i < 4; i++) {
-        const float sxr = __ldg(a.t.wsyn_xr + x + i), sxl = __ldg(a.t.wsyn_xl + x + i);
-        v[i] = ((comp(aa, i) * sxr + comp(b, i) * sxl) * wr + (comp(c, i) * sxr + comp(d, i) * sxl) * wl) + a.rounder +
-               a.base;
-      }
-    }
-  }
-  const int fr = field_row(k, g.H, g.interlaced);
-  if (!FFT3D_IN(fr >= 0 && fr < g.H && x0 + 3 < g.W, a.err)) return;
-  T* row = reinterpret_cast<T*>(static_cast<char*>(a.dst) + (long long)fr * a.dst_stride);
-  typename Pack4<T>::V o;
-  o.x = clamp_sample<T>(v[0], a.maxval);
-  o.y = clamp_sample<T>(v[1], a.maxval);
-  o.z = clamp_sample<T>(v[2], a.maxval);
-  o.w = clamp_sample<T>(v[3], a.maxval);
-  *reinterpret_cast<typename Pack4<T>::V*>(row + x0) = o;
-}
-
 constexpr int kOlaTx = 32, kOlaTy = 8;
 
 template <typename T>
@@ -320,9 +159,10 @@ cudaError_t launch_filter_bins(const InverseArgs& a, float2* F, int mode, cudaSt
   return cudaGetLastError();
 }
 
-cudaError_t launch_filter_inverse_group(const InverseArgs& a, const TemporalSet& ts, int mode, cudaStream_t s) {
+cudaError_t launch_filter_inverse_group(const InverseArgs& a, const TemporalSet& ts, int mode, cudaStream_t s,
+                                        const OlaFuse* of) {
   const SizeEntry* e = find_size(a.g.bw, a.g.bh);
-  return e ? e->inv_group(a, ts, mode, s) : cudaErrorInvalidValue;
+  return e ? e->inv_group(a, ts, mode, s, of) : cudaErrorInvalidValue;
 }
 
 cudaError_t launch_filter_frames(const InverseArgs& a, const FilterFrameSet& fs, int mode, cudaStream_t s) {

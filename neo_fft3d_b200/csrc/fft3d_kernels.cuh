@@ -197,6 +197,26 @@ struct OlaArgs {
   int* err;               // device error flag (bounds-checked build), or null
 };
 
+// Overlap-add fused into a run's filter/inverse launch (k_filter_inverse_group).
+// Output tile (tx, ty), 1 <= tx <= tiles_x, 1 <= ty <= tiles_y, is the pixels
+// x0 in [(tx-1)*sx, tx*sx), k in [(ty-1)*sy, ty*sy) of the processed region,
+// whose blocks are (tx, ty), (tx-1, ty) when ow > 0, (tx, ty-1) when oh > 0
+// and (tx-1, ty-1) when both. Each CTA adds one arrival to the counter of
+// every tile its block feeds once its time-domain blocks are stored; the CTA
+// that brings a counter to the tile's block count times the launch's epoch
+// (so the counters need no reset between launches) does that tile's
+// overlap-add for all the run's frames, from L2.
+struct OlaFuse {
+  OlaArgs o;                      // shared arguments (o.tdom, o.dst unused)
+  void* dst[kGroupTile];          // frame j's destination plane at the crop origin
+  long long dst_stride[kGroupTile];
+  unsigned* cnt;                  // arrival counters, indexed ty * nox + tx
+  unsigned epoch;                 // this launch's epoch (> 0)
+  int tiles_x, tiles_y;
+  int bytes;                      // sample size: 1, 2 or 4
+  int px4;                        // 4-pixel form (the plane meets its rules)
+};
+
 // One batched launch: `nitems` work items (plane index into `args`, CTA of
 // that plane) walked by a grid of `grid` CTAs; args/items in device memory.
 struct BatchLaunch {
@@ -224,7 +244,9 @@ cudaError_t launch_filter_inverse(const InverseArgs& a, int mode, cudaStream_t s
 cudaError_t launch_filter_inverse_frames(const InverseArgs& a, const FrameSet& fs, int mode, cudaStream_t s);
 // A run of frames of one plane in one launch, each block's spectra read once
 // for the whole run (modes -1..5; Kalman runs in frame order).
-cudaError_t launch_filter_inverse_group(const InverseArgs& a, const TemporalSet& ts, int mode, cudaStream_t s);
+// With `of`, the run's overlap-adds are done by the same launch (OlaFuse).
+cudaError_t launch_filter_inverse_group(const InverseArgs& a, const TemporalSet& ts, int mode, cudaStream_t s,
+                                        const OlaFuse* of = nullptr);
 // Forward transforms of fs.count frames of one plane in one launch; a holds
 // what they share (geometry, windows, sample offset).
 cudaError_t launch_forward_frames(const ForwardArgs& a, const FwdFrameSet& fs, int bytes_per_sample, cudaStream_t s);

@@ -15,6 +15,15 @@ namespace {
 
 constexpr int kWarps = 4;       // warps per CTA in k_forward / k_filter_inverse
 
+// CTAs per SM that the frame-group forward and filter/inverse kernels are
+// compiled for (their register budget: 65536 / (128 x this))
+#ifndef FFT3D_FWD_CTAS
+#define FFT3D_FWD_CTAS 5
+#endif
+#ifndef FFT3D_GROUP_CTAS
+#define FFT3D_GROUP_CTAS 5
+#endif
+
 // reflect-101 of index s into [0, n): the cover's mirror margins
 // (src/buffer.cpp:19-26, 65-79); repeated for planes narrower than a margin.
 __device__ __forceinline__ int reflect101(int s, int n) {
@@ -360,7 +369,7 @@ __global__ void __launch_bounds__(kWarps * 32, 5) k_forward(ForwardArgs a) {
 // x % fs.ctas of frame x / fs.ctas (one launch instead of one per frame, so
 // the grid has no per-frame wave tail).
 template <int BW, int BH, typename T>
-__global__ void __launch_bounds__(kWarps * 32, 5) k_forward_frames(ForwardArgs a, FwdFrameSet fs) {
+__global__ void __launch_bounds__(kWarps * 32, FFT3D_FWD_CTAS) k_forward_frames(ForwardArgs a, FwdFrameSet fs) {
   const int j = blockIdx.x / fs.ctas, c = blockIdx.x - j * fs.ctas;
   FrameFwd w{nullptr, 0, nullptr};
 #pragma unroll
@@ -920,6 +929,217 @@ __global__ void __launch_bounds__(kWarps * 32) k_filter_inverse_batch(const Inve
   }
 }
 
+// ---------------------------------------------------------------- overlap-add pixels
+
+// Time-domain block reads of the overlap-add. Blocks written by an earlier
+// launch go through the read-only path without L1 allocation (each value is
+// read once; the synthesis windows stay in L1). Blocks written by other CTAs
+// of the same launch (L2 = true, the fused overlap-add of a frame group) are
+// read at L2, the point where those CTAs' stores are visible.
+template <bool L2>
+__device__ __forceinline__ float ld_tdom(const float* p) {
+  if constexpr (L2) return __ldcg(p);
+  else return __ldg(p);
+}
+template <bool L2>
+__device__ __forceinline__ float4 ld_tdom4(const float* p) {
+  if constexpr (L2) {
+    return __ldcg(reinterpret_cast<const float4*>(p));
+  } else {
+    float4 q;
+    asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+        : "=f"(q.x), "=f"(q.y), "=f"(q.z), "=f"(q.w)
+        : "l"(p));
+    return q;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void store_sample(T* p, float v, int maxval);
+template <>
+__device__ __forceinline__ void store_sample<uint8_t>(uint8_t* p, float v, int maxval) {
+  int i = __float2int_rz(v);  // C cast: truncation toward zero (src/buffer.cpp:406)
+  i = i < 0 ? 0 : (i > maxval ? maxval : i);
+  *p = (uint8_t)i;
+}
+template <>
+__device__ __forceinline__ void store_sample<uint16_t>(uint16_t* p, float v, int maxval) {
+  int i = __float2int_rz(v);
+  i = i < 0 ? 0 : (i > maxval ? maxval : i);
+  *p = (uint16_t)i;
+}
+template <>
+__device__ __forceinline__ void store_sample<float>(float* p, float v, int) {
+  float c = v < 0.f ? 0.f : v;  // float samples clamp to [0, 1] (src/buffer.cpp:397)
+  *p = c > 1.f ? 1.f : c;
+}
+
+// One thread per output pixel of the processed region: the (at most four)
+// blocks covering it, weighted with the synthesis windows and the FFT
+// normalisation in the association order of src/buffer.cpp:399-559.
+template <typename T, bool L2 = false>
+__device__ __forceinline__ void overlap_add_px(const OlaArgs& a, int x0, int k) {
+  const Geom& g = a.g;
+  if (x0 >= g.W || k >= g.H) return;
+  const int Y = g.sy + k, X = g.sx + x0;
+  const int by = Y / g.sy, y = Y - by * g.sy;
+  const int bx = X / g.sx, x = X - bx * g.sx;
+  const bool yov = y < g.oh, xov = x < g.ow;
+  const int bw = g.bw, bh = g.bh;
+  auto at = [&](int bxx, int byy, int yy, int xx) {
+    if (!FFT3D_IN(bxx >= 0 && bxx < g.nox && byy >= 0 && byy < g.noy && yy >= 0 && yy < bh && xx >= 0 && xx < bw,
+                  a.err))
+      return 0.f;
+    return ld_tdom<L2>(a.tdom + ((size_t)(byy * g.nox + bxx) * bh + yy) * bw + xx);
+  };
+  const float norm = a.norm;
+  float v;
+  if (!yov) {
+    const float d = at(bx, by, y, x);
+    if (!xov) v = d * norm + a.rounder + a.base;
+    else {
+      const float c = at(bx - 1, by, y, x + g.sx);
+      v = (c * __ldg(a.t.wsyn_xr + x) + d * __ldg(a.t.wsyn_xl + x)) * norm + a.rounder + a.base;
+    }
+  } else {
+    const float wr = __ldg(a.t.wsyn_yr + y) * norm, wl = __ldg(a.t.wsyn_yl + y) * norm;
+    const float b = at(bx, by - 1, y + g.sy, x), d = at(bx, by, y, x);
+    if (!xov) v = (b * wr + d * wl) + a.rounder + a.base;
+    else {
+      const float aa = at(bx - 1, by - 1, y + g.sy, x + g.sx), c = at(bx - 1, by, y, x + g.sx);
+      const float sxr = __ldg(a.t.wsyn_xr + x), sxl = __ldg(a.t.wsyn_xl + x);
+      v = ((aa * sxr + b * sxl) * wr + (c * sxr + d * sxl) * wl) + a.rounder + a.base;
+    }
+  }
+  const int fr = field_row(k, g.H, g.interlaced);
+  if (!FFT3D_IN(fr >= 0 && fr < g.H, a.err)) return;
+  T* row = reinterpret_cast<T*>(static_cast<char*>(a.dst) + (long long)fr * a.dst_stride);
+  store_sample<T>(row + x0, v, a.maxval);
+}
+
+// Four adjacent output pixels per thread (x0 a multiple of 4), for planes
+// whose block step, overlap, width and block width are multiples of 4 and
+// whose destination rows are aligned for a 4-sample store: the four pixels
+// share their blocks and overlap case, so the tdom reads are float4 loads,
+// the block indices are computed once and the samples go out in one store.
+// Each pixel's arithmetic is overlap_add_px's, term for term.
+template <typename T>
+struct Pack4;
+template <>
+struct Pack4<uint8_t> {
+  using V = uchar4;
+};
+template <>
+struct Pack4<uint16_t> {
+  using V = ushort4;
+};
+template <>
+struct Pack4<float> {
+  using V = float4;
+};
+
+template <typename T>
+__device__ __forceinline__ T clamp_sample(float v, int maxval) {
+  if constexpr (sizeof(T) == 4) {
+    float c = v < 0.f ? 0.f : v;
+    return c > 1.f ? 1.f : c;
+  } else {
+    int i = __float2int_rz(v);
+    i = i < 0 ? 0 : (i > maxval ? maxval : i);
+    return (T)i;
+  }
+}
+
+// The 4-pixel overlap-add in two steps, so that a thread can issue the block
+// reads of several pixel quads before it computes any of them: ola4_fetch
+// reads the (at most four) time-domain float4s of quad (x0, k) from `tdom`,
+// ola4_finish weights, sums, rounds and stores them.
+struct Ola4Px {
+  float4 aa, b, c, d;  // blocks (bx-1, by-1), (bx, by-1), (bx-1, by), (bx, by); zero where not read
+  int x, y;            // position inside the block step
+  bool xov, yov, ok;
+};
+
+template <bool L2>
+__device__ __forceinline__ Ola4Px ola4_fetch(const OlaArgs& a, const float* tdom, int x0, int k) {
+  const Geom& g = a.g;
+  Ola4Px p;
+  p.aa = p.b = p.c = p.d = make_float4(0.f, 0.f, 0.f, 0.f);
+  p.ok = x0 < g.W && k < g.H;
+  if (!p.ok) return p;
+  const int Y = g.sy + k, X = g.sx + x0;
+  const int by = Y / g.sy, bx = X / g.sx;
+  p.y = Y - by * g.sy;
+  p.x = X - bx * g.sx;
+  p.yov = p.y < g.oh;
+  p.xov = p.x < g.ow;
+  const int bw = g.bw, bh = g.bh;
+  auto at4 = [&](int bxx, int byy, int yy, int xx) {
+    if (!FFT3D_IN(bxx >= 0 && bxx < g.nox && byy >= 0 && byy < g.noy && yy >= 0 && yy < bh && xx >= 0 &&
+                      xx + 3 < bw,
+                  a.err))
+      return make_float4(0.f, 0.f, 0.f, 0.f);
+    return ld_tdom4<L2>(tdom + ((size_t)(byy * g.nox + bxx) * bh + yy) * bw + xx);
+  };
+  p.d = at4(bx, by, p.y, p.x);
+  if (p.xov) p.c = at4(bx - 1, by, p.y, p.x + g.sx);
+  if (p.yov) {
+    p.b = at4(bx, by - 1, p.y + g.sy, p.x);
+    if (p.xov) p.aa = at4(bx - 1, by - 1, p.y + g.sy, p.x + g.sx);
+  }
+  return p;
+}
+
+template <typename T>
+__device__ __forceinline__ void ola4_finish(const OlaArgs& a, void* dst, long long dst_stride, int x0, int k,
+                                            const Ola4Px& p) {
+  if (!p.ok) return;
+  const Geom& g = a.g;
+  const int x = p.x, y = p.y;
+  auto comp = [](const float4& q, int i) { return i == 0 ? q.x : (i == 1 ? q.y : (i == 2 ? q.z : q.w)); };
+  const float norm = a.norm;
+  float v[4];
+  if (!p.yov) {
+    if (!p.xov) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) v[i] = comp(p.d, i) * norm + a.rounder + a.base;
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+        v[i] = (comp(p.c, i) * __ldg(a.t.wsyn_xr + x + i) + comp(p.d, i) * __ldg(a.t.wsyn_xl + x + i)) * norm +
+               a.rounder + a.base;
+    }
+  } else {
+    const float wr = __ldg(a.t.wsyn_yr + y) * norm, wl = __ldg(a.t.wsyn_yl + y) * norm;
+    if (!p.xov) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) v[i] = (comp(p.b, i) * wr + comp(p.d, i) * wl) + a.rounder + a.base;
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const float sxr = __ldg(a.t.wsyn_xr + x + i), sxl = __ldg(a.t.wsyn_xl + x + i);
+        v[i] = ((comp(p.aa, i) * sxr + comp(p.b, i) * sxl) * wr + (comp(p.c, i) * sxr + comp(p.d, i) * sxl) * wl) +
+               a.rounder + a.base;
+      }
+    }
+  }
+  const int fr = field_row(k, g.H, g.interlaced);
+  if (!FFT3D_IN(fr >= 0 && fr < g.H && x0 + 3 < g.W, a.err)) return;
+  T* row = reinterpret_cast<T*>(static_cast<char*>(dst) + (long long)fr * dst_stride);
+  typename Pack4<T>::V o;
+  o.x = clamp_sample<T>(v[0], a.maxval);
+  o.y = clamp_sample<T>(v[1], a.maxval);
+  o.z = clamp_sample<T>(v[2], a.maxval);
+  o.w = clamp_sample<T>(v[3], a.maxval);
+  *reinterpret_cast<typename Pack4<T>::V*>(row + x0) = o;
+}
+
+template <typename T, bool L2 = false>
+__device__ __forceinline__ void overlap_add_px4(const OlaArgs& a, int x0, int k) {
+  const Ola4Px p = ola4_fetch<L2>(a, a.tdom, x0, k);
+  ola4_finish<T>(a, a.dst, a.dst_stride, x0, k, p);
+}
+
 // ---------------------------------------------------------------- frame groups, one CTA per block
 
 // Dynamic shared memory of k_filter_inverse_group: two grid fractions per
@@ -1060,8 +1280,49 @@ __device__ __forceinline__ void group_filter_one(const InverseArgs& a, const Tem
   if (bin == 0) gsh[j] = a.c.degrid * v0.x / gs0;
 }
 
+// The overlap-add of output tile (tx, ty) (OlaFuse) for the run's frames:
+// overlap_add_px4 / overlap_add_px per pixel, the blocks read from L2.
+template <typename T>
+__device__ __noinline__ void group_ola_tile(const OlaFuse& of, const TemporalSet& ts, int count, int tx, int ty) {
+  const Geom& g = of.o.g;
+  const int x_lo = (tx - 1) * g.sx, y_lo = (ty - 1) * g.sy;
+  const int wd = min(g.sx, g.W - x_lo), ht = min(g.sy, g.H - y_lo);
+  if (of.px4) {
+    // quads (frame j, row yy, quad xx); each thread fetches K of them before
+    // it finishes any, so that their L2 reads overlap
+    constexpr int K = 2;
+    const int q = (wd + 3) / 4, per = q * ht, total = count * per;
+    for (int i0 = threadIdx.x; i0 < total; i0 += K * blockDim.x) {
+      Ola4Px p[K];
+      int jj[K], xs[K], ks[K];
+#pragma unroll
+      for (int u = 0; u < K; u++) {
+        const int i = i0 + u * blockDim.x;
+        const int j = i < total ? i / per : 0, r = i - j * per, yy = r / q, xx = r - yy * q;
+        jj[u] = j;
+        xs[u] = i < total ? x_lo + 4 * xx : g.W;  // out of range: fetch and finish skip it
+        ks[u] = y_lo + yy;
+        p[u] = ola4_fetch<true>(of.o, ts.tdom[j], xs[u], ks[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < K; u++) ola4_finish<T>(of.o, of.dst[jj[u]], of.dst_stride[jj[u]], xs[u], ks[u], p[u]);
+    }
+    return;
+  }
+  const int per = wd * ht;
+  for (int i = threadIdx.x; i < count * per; i += blockDim.x) {
+    const int j = i / per, r = i - j * per, yy = r / wd, xx = r - yy * wd;
+    OlaArgs b = of.o;
+    b.tdom = ts.tdom[j];
+    b.dst = of.dst[j];
+    b.dst_stride = of.dst_stride[j];
+    overlap_add_px<T, true>(b, x_lo + xx, y_lo + yy);
+  }
+}
+
 template <int BW, int BH, int MODE>
-__device__ __forceinline__ void filter_inverse_group_cta(const InverseArgs& a, const TemporalSet& ts, int blk) {
+__device__ __forceinline__ void filter_inverse_group_cta(const InverseArgs& a, const TemporalSet& ts, int blk,
+                                                         const OlaFuse* of = nullptr) {
   constexpr int NH = BW / 2 + 1, HC = BW / 2, BINS = BH * NH, PAIRS = BINS / 2, NT = kWarps * 32;
   static_assert(BINS % 2 == 0, "bin pairs");
   extern __shared__ float2 smem2[];
@@ -1143,12 +1404,42 @@ __device__ __forceinline__ void filter_inverse_group_cta(const InverseArgs& a, c
     if (FFT3D_IN(ts.tdom[j] != nullptr && blk < a.g.nblocks, a.err))
       reinterpret_cast<float2*>(ts.tdom[j] + (size_t)blk * BH * BW)[r] = S[j * BINS + y * NH + x];
   }
+  // 6. the overlap-adds of the output tiles whose last block this is (OlaFuse):
+  //    release (a barrier after the stores, then a fence before each tile
+  //    arrival), acquire (a fence after the arrival that completes a tile,
+  //    then a barrier); no waiting
+  if (of) {
+    __shared__ int done[4];
+    __syncthreads();  // the CTA's stores precede the arrivals below (the fence there is cumulative)
+    const int bx = blk % a.g.nox, by = blk / a.g.nox;
+    if (t < 4) {
+      const int dx = t & 1, dy = t >> 1, tx = bx + dx, ty = by + dy;
+      const unsigned need = (a.g.ow > 0 ? 2u : 1u) * (a.g.oh > 0 ? 2u : 1u);
+      int last = 0;
+      if ((dx == 0 || a.g.ow > 0) && (dy == 0 || a.g.oh > 0) && tx >= 1 && tx <= of->tiles_x && ty >= 1 &&
+          ty <= of->tiles_y && FFT3D_IN(tx < a.g.nox && ty < a.g.noy, a.err)) {
+        __threadfence();
+        last = atomicAdd(of->cnt + ty * a.g.nox + tx, 1u) + 1u == need * of->epoch;
+        if (last) __threadfence();
+      }
+      done[t] = last;
+    }
+    __syncthreads();
+    for (int q = 0; q < 4; q++) {
+      if (!done[q]) continue;
+      const int tx = bx + (q & 1), ty = by + (q >> 1);
+      if (of->bytes == 1) group_ola_tile<uint8_t>(*of, ts, count, tx, ty);
+      else if (of->bytes == 2) group_ola_tile<uint16_t>(*of, ts, count, tx, ty);
+      else group_ola_tile<float>(*of, ts, count, tx, ty);
+    }
+  }
 }
 
 template <int BW, int BH, int MODE>
-__global__ void __launch_bounds__(kWarps * 32, 5) k_filter_inverse_group(InverseArgs a,
-                                                                     const __grid_constant__ TemporalSet ts) {
-  filter_inverse_group_cta<BW, BH, MODE>(a, ts, blockIdx.x);
+__global__ void __launch_bounds__(kWarps * 32, FFT3D_GROUP_CTAS) k_filter_inverse_group(InverseArgs a,
+                                                                     const __grid_constant__ TemporalSet ts,
+                                                                     const __grid_constant__ OlaFuse of) {
+  filter_inverse_group_cta<BW, BH, MODE>(a, ts, blockIdx.x, of.cnt ? &of : nullptr);
 }
 
 // Batched runs of many planes: work item (run, block of that run's plane). The
@@ -1505,25 +1796,33 @@ cudaError_t inv_frames(const InverseArgs& a, const FrameSet& fs, int mode, cudaS
 }
 
 template <int BW, int BH, int MODE>
-cudaError_t inv_group_mode(const InverseArgs& a, const TemporalSet& ts, cudaStream_t s) {
+cudaError_t inv_group_mode(const InverseArgs& a, const TemporalSet& ts, const OlaFuse& of, cudaStream_t s) {
   const int smem = group_smem_bytes<BW, BH>(kGroupTile);
   cudaError_t e = fft3d::smem_attr(k_filter_inverse_group<BW, BH, MODE>, smem);
   if (e != cudaSuccess) return e;
-  k_filter_inverse_group<BW, BH, MODE><<<a.g.nblocks, kWarps * 32, group_smem_bytes<BW, BH>(ts.count), s>>>(a, ts);
+  k_filter_inverse_group<BW, BH, MODE>
+      <<<a.g.nblocks, kWarps * 32, group_smem_bytes<BW, BH>(ts.count), s>>>(a, ts, of);
   return cudaGetLastError();
 }
 
 template <int BW, int BH>
-cudaError_t inv_group(const InverseArgs& a, const TemporalSet& ts, int mode, cudaStream_t s) {
+cudaError_t inv_group(const InverseArgs& a, const TemporalSet& ts, int mode, cudaStream_t s, const OlaFuse* ofp) {
   if (ts.count < 1 || ts.count > kGroupTile) return cudaErrorInvalidValue;
+  OlaFuse of{};
+  if (ofp) {
+    of = *ofp;
+    if (!of.cnt || of.epoch == 0 || of.tiles_x < 1 || of.tiles_y < 1 || of.tiles_x >= a.g.nox ||
+        of.tiles_y >= a.g.noy || (of.bytes != 1 && of.bytes != 2 && of.bytes != 4))
+      return cudaErrorInvalidValue;
+  }
   switch (mode) {
-    case MODE_SHARPEN_ONLY: return inv_group_mode<BW, BH, MODE_SHARPEN_ONLY>(a, ts, s);
-    case MODE_KALMAN: return inv_group_mode<BW, BH, MODE_KALMAN>(a, ts, s);
-    case 1: return inv_group_mode<BW, BH, 1>(a, ts, s);
-    case 2: return inv_group_mode<BW, BH, 2>(a, ts, s);
-    case 3: return inv_group_mode<BW, BH, 3>(a, ts, s);
-    case 4: return inv_group_mode<BW, BH, 4>(a, ts, s);
-    case 5: return inv_group_mode<BW, BH, 5>(a, ts, s);
+    case MODE_SHARPEN_ONLY: return inv_group_mode<BW, BH, MODE_SHARPEN_ONLY>(a, ts, of, s);
+    case MODE_KALMAN: return inv_group_mode<BW, BH, MODE_KALMAN>(a, ts, of, s);
+    case 1: return inv_group_mode<BW, BH, 1>(a, ts, of, s);
+    case 2: return inv_group_mode<BW, BH, 2>(a, ts, of, s);
+    case 3: return inv_group_mode<BW, BH, 3>(a, ts, of, s);
+    case 4: return inv_group_mode<BW, BH, 4>(a, ts, of, s);
+    case 5: return inv_group_mode<BW, BH, 5>(a, ts, of, s);
   }
   return cudaErrorInvalidValue;
 }

@@ -24,7 +24,7 @@ struct SizeEntry {
   // and their new frames' forward transforms in one launch
   cudaError_t (*fwd_frames)(const ForwardArgs&, const FwdFrameSet&, int bytes_per_sample, cudaStream_t);
   // a run of frames filtered and inverse-transformed with one CTA per block
-  cudaError_t (*inv_group)(const InverseArgs&, const TemporalSet&, int mode, cudaStream_t);
+  cudaError_t (*inv_group)(const InverseArgs&, const TemporalSet&, int mode, cudaStream_t, const OlaFuse*);
   // and its batched form over the runs of many planes
   cudaError_t (*inv_group_batch)(const BatchLaunch&, int mode, cudaStream_t);
 };

@@ -52,7 +52,7 @@ def _per_frame(torch, planes, dev, clip, filt):
     engs = _engines(planes, clip, filt)
     outs = []
     for e, a in zip(engs, dev):
-        o = torch.empty_like(a)
+        o = torch.full_like(a, 1)  # a value no filtered sample takes: unwritten pixels show
         st = a.shape[2] * a.element_size()
         for n in range(F):
             e.filter_device(n, [_ptr(a, n + d) for d in range(-2, 3)], [st] * 5, _ptr(o, n), st, 0)
@@ -67,7 +67,7 @@ def _grouped(torch, planes, dev, clip, filt, sizes):
     engs = _engines(planes, clip, filt)
     outs = []
     for e, a in zip(engs, dev):
-        o = torch.empty_like(a)
+        o = torch.full_like(a, 1)  # a value no filtered sample takes: unwritten pixels show
         st = a.shape[2] * a.element_size()
         n0, i = 0, 0
         while n0 < F:
@@ -120,7 +120,7 @@ def test_frame_group_timing_counts_unique_spectra(gpu):
     planes, dev = _clip(torch, clip)
     e = _engines(planes[:1], clip, filt)[0]
     a = dev[0]
-    o = torch.empty_like(a)
+    o = torch.full_like(a, 1)  # a value no filtered sample takes: unwritten pixels show
     st = a.shape[2]
     e.filter_frames_device(4, [_ptr(a, n) for n in range(2, 12)], [st] * 10, [_ptr(o, n) for n in range(4, 10)],
                            [st] * 6, 0)  # warm: frames 4..9
@@ -255,7 +255,7 @@ def test_reset_waits_for_queued_work(gpu, grouped):
     st = a.shape[2]
     outs = []
     for _ in range(3):
-        o = torch.empty_like(a)
+        o = torch.full_like(a, 1)  # a value no filtered sample takes: unwritten pixels show
         e.reset()
         if grouped:
             for n0 in range(0, F, 8):
