@@ -36,6 +36,7 @@ std::vector<SizeEntry>& table() {
 }
 
 constexpr int kOlaTx = 32, kOlaTy = 8;
+constexpr int kOla4BatchRows = 4 * kOlaTy;  // rows of one batched 4-pixel overlap-add item
 
 template <typename T>
 __global__ void __launch_bounds__(kOlaTx * kOlaTy) k_overlap_add4(OlaArgs a) {
@@ -86,7 +87,11 @@ __global__ void __launch_bounds__(kOlaTx * kOlaTy) k_overlap_add4_batch(const Ol
     const OlaArgs a = args[it.x];  // private copy: fields stay in registers
     const int tx = (a.g.W + 4 * kOlaTx - 1) / (4 * kOlaTx);
     const int ty = it.y / tx, t = it.y - ty * tx;
-    overlap_add_px4<T>(a, 4 * (t * kOlaTx + threadIdx.x), ty * kOlaTy + threadIdx.y);
+    // kOla4BatchRows rows per item, so that the argument loads are shared by
+    // several pixel quads per thread
+#pragma unroll
+    for (int r = 0; r < kOla4BatchRows; r += kOlaTy)
+      overlap_add_px4<T>(a, 4 * (t * kOlaTx + threadIdx.x), ty * kOla4BatchRows + r + threadIdx.y);
   }
 }
 
@@ -280,7 +285,7 @@ int batch_items_overlap_add(const Geom& g) {
 }
 
 int batch_items_overlap_add4(const Geom& g) {
-  return ((g.W + 4 * kOlaTx - 1) / (4 * kOlaTx)) * ((g.H + kOlaTy - 1) / kOlaTy);
+  return ((g.W + 4 * kOlaTx - 1) / (4 * kOlaTx)) * ((g.H + kOla4BatchRows - 1) / kOla4BatchRows);
 }
 
 bool batch_overlap_add4_ok(const OlaArgs& a, int bytes) {

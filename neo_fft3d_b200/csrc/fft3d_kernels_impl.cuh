@@ -395,7 +395,9 @@ __global__ void __launch_bounds__(kWarps * 32, ctas_for(FFT3D_FWD_CTAS, kWarps *
 // Batched forward: work item i = (plane, CTA of that plane); the grid walks
 // the items (persistent when the grid is smaller than the item count).
 template <int BW, int BH, typename T>
-__global__ void __launch_bounds__(kWarps * 32, 5) k_forward_batch(const ForwardArgs* __restrict__ args,
+__global__ void __launch_bounds__(kWarps * 32,
+                                  ctas_for(FFT3D_FWD_CTAS, kWarps * fft_smem_bytes<BW, BH>() + (int)sizeof(ForwardArgs)))
+    k_forward_batch(const ForwardArgs* __restrict__ args,
                                                                  const int2* __restrict__ items, int nitems) {
   // the item's arguments staged in shared memory: the body's stores cannot
   // alias them, they cost no registers, and the body can take the per-plane
@@ -1458,7 +1460,9 @@ __global__ void __launch_bounds__(kWarps * 32, ctas_for(FFT3D_GROUP_CTAS, group_
 // stores cannot alias them (a reference into global memory would be reloaded
 // after every store) and they cost no registers.
 template <int BW, int BH, int MODE>
-__global__ void __launch_bounds__(kWarps * 32, 5) k_filter_inverse_group_batch(const GroupRun* __restrict__ runs,
+__global__ void __launch_bounds__(kWarps * 32,
+                                  ctas_for(FFT3D_GROUP_CTAS, group_smem_bytes<BW, BH>(kGroupTile) + (int)sizeof(GroupRun)))
+    k_filter_inverse_group_batch(const GroupRun* __restrict__ runs,
                                                                            const int2* __restrict__ items,
                                                                            int nitems) {
   extern __shared__ float2 smem2[];
