@@ -458,11 +458,11 @@ __device__ __forceinline__ float dehalo_fact(const InverseArgs& a, float psd, fl
 // limited Wiener factor applied to one temporal component, code_impl_C.h:34-40:
 // max((psd - noise) / psd, lowlimit) as max(1 - noise / psd, lowlimit) with
 // the fast reciprocal (<= 2 ulp, far inside the +-1 LSB output bar)
-__device__ __forceinline__ void wiener(float& re, float& im, float noise, float lowlimit) {
-  const float q = fmaf(-noise, __fdividef(1.f, bin_psd(re, im)), 1.f);
+// (both parts scaled by one packed multiply)
+__device__ __forceinline__ void wiener(float2& v, float noise, float lowlimit) {
+  const float q = fmaf(-noise, __fdividef(1.f, bin_psd(v.x, v.y)), 1.f);
   const float f = fmaxf(q, lowlimit);
-  re *= f;
-  im *= f;
+  v = __fmul2_rn(v, make_float2(f, f));
 }
 
 // Learned noise power of bin `bin` of the block at spectrum offset `off`.
@@ -549,7 +549,7 @@ __device__ __forceinline__ float2 filter_vals(const InverseArgs& a, const float2
     if (a.c.degrid != 0.f) g = __fmul2_rn(tb.grid, make_float2(gk, gk));
     const float noise = a.psd ? learned_noise(a, off, bin) : a.c.pattern ? __ldg(a.t.pattern3d + bin) : a.c.sigma2n;
     const float ll = a.c.lowlimit;
-    auto wf = [&](float2& v) { wiener(v.x, v.y, noise, ll); };
+    auto wf = [&](float2& v) { wiener(v, noise, ll); };
     auto add = [](float2 x, float2 y) { return __fadd2_rn(x, y); };
     auto sub = [](float2 x, float2 y) { return __fadd2_rn(x, make_float2(-y.x, -y.y)); };
     auto rot = [](float2 v) { return make_float2(v.y, -v.x); };  // -i v
@@ -624,16 +624,17 @@ __device__ __forceinline__ float2 filter_bin(const InverseArgs& a, size_t off, i
 }
 
 // separate sharpen/dehalo pass on a filtered bin, src/code_impl/Sharpen.cpp:13-63
+// (the grid term removed and restored with packed f32x2 operations)
 __device__ __forceinline__ float2 sharpen_bin(const InverseArgs& a, float2 v, const BinTab& tb, float gf) {
   float2 gc = make_float2(0.f, 0.f);
-  if (a.c.degrid != 0.f) gc = make_float2(gf * tb.grid.x, gf * tb.grid.y);
-  const float cr = v.x - gc.x, ci = v.y - gc.y;
-  const float psd = bin_psd(cr, ci);
+  if (a.c.degrid != 0.f) gc = __fmul2_rn(tb.grid, make_float2(gf, gf));
+  const float2 c = __fadd2_rn(v, make_float2(-gc.x, -gc.y));
+  const float psd = bin_psd(c.x, c.y);
   float f;
   if (a.c.use_sharpen && a.c.use_dehalo) f = sharpen_fact(a, psd, tb.wsh) * dehalo_fact(a, psd, tb.wdh);
   else if (a.c.use_sharpen) f = sharpen_fact(a, psd, tb.wsh);
   else f = dehalo_fact(a, psd, tb.wdh);
-  return make_float2(cr * f + gc.x, ci * f + gc.y);
+  return __ffma2_rn(c, make_float2(f, f), gc);
 }
 
 // ---------------------------------------------------------------- filter (streaming)
