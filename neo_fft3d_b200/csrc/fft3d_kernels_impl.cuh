@@ -463,6 +463,23 @@ __device__ __forceinline__ BinTab bin_tab(const InverseArgs& a, int bin) {
   return t;
 }
 
+// The hardware's approximate reciprocal and reciprocal square root (PTX
+// rcp.approx / rsqrt.approx, the instructions __fdividef and rsqrtf stand on).
+// Every caller's argument is a normal float (a power spectrum plus 1e-15,
+// a noise power of at least 1e-15, a ratio clamped to >= 1e-30), where the
+// .ftz forms give the same result without the handling of denormal
+// arguments that the plain forms carry.
+__device__ __forceinline__ float rcp_nrm(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rsqrt_nrm(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // |c|^2 + 1e-15 of a bin (the reference's psd, src/code_impl/Apply.cpp:27-31)
 __device__ __forceinline__ float bin_psd(float re, float im) { return fmaf(re, re, fmaf(im, im, 1.0e-15f)); }
 
@@ -472,12 +489,12 @@ __device__ __forceinline__ float sharpen_fact(const InverseArgs& a, float psd, f
   // first as in the reference (the product of its terms overflows float for
   // high bit depths), its square root as r * rsqrt(r) (the clamp keeps r = 0,
   // i.e. smax = 0, finite)
-  const float r = __fdividef(psd * a.c.smax2n, (psd + a.c.smin2n) * (psd + a.c.smax2n));
-  return fmaf(a.c.sharpen * wsh, r * rsqrtf(fmaxf(r, 1e-30f)), 1.f);
+  const float r = psd * a.c.smax2n * rcp_nrm((psd + a.c.smin2n) * (psd + a.c.smax2n));
+  return fmaf(a.c.sharpen * wsh, r * rsqrt_nrm(fmaxf(r, 1e-30f)), 1.f);
 }
 __device__ __forceinline__ float dehalo_fact(const InverseArgs& a, float psd, float wdh) {
   // src/code_impl/Apply.cpp:132
-  return __fdividef(psd + a.c.ht2n, (psd + a.c.ht2n) + a.c.dehalo * wdh * psd);
+  return (psd + a.c.ht2n) * rcp_nrm((psd + a.c.ht2n) + a.c.dehalo * wdh * psd);
 }
 
 // limited Wiener factor applied to one temporal component, code_impl_C.h:34-40:
@@ -485,7 +502,7 @@ __device__ __forceinline__ float dehalo_fact(const InverseArgs& a, float psd, fl
 // the fast reciprocal (<= 2 ulp, far inside the +-1 LSB output bar)
 // (both parts scaled by one packed multiply)
 __device__ __forceinline__ void wiener(float2& v, float noise, float lowlimit) {
-  const float q = fmaf(-noise, __fdividef(1.f, bin_psd(v.x, v.y)), 1.f);
+  const float q = fmaf(-noise, rcp_nrm(bin_psd(v.x, v.y)), 1.f);
   const float f = fmaxf(q, lowlimit);
   v = __fmul2_rn(v, make_float2(f, f));
 }
@@ -508,7 +525,7 @@ __device__ __forceinline__ void kalman_step(const InverseArgs& a, float2 cur, fl
     last = cur;
   } else {
     const float sum = cv + cp;
-    const float gain = __fdividef(sum, sum + sigma);
+    const float gain = sum * rcp_nrm(sum + sigma);
     cp = gain * gain * sigma;
     cv = (1.f - gain) * sum;
     last.x = gain * cur.x + (1.f - gain) * last.x;
@@ -555,7 +572,7 @@ __device__ __forceinline__ float2 filter_vals(const InverseArgs& a, const float2
     const float cr = cur.x - gc.x, ci = cur.y - gc.y;
     const float psd = bin_psd(cr, ci);
     const float noise = a.psd ? learned_noise(a, off, bin) : a.c.pattern ? __ldg(a.t.pattern2d + bin) : a.c.sigma2n;
-    float f = fmaxf(fmaf(-noise, __fdividef(1.f, psd), 1.f), a.c.lowlimit);
+    float f = fmaxf(fmaf(-noise, rcp_nrm(psd), 1.f), a.c.lowlimit);
     if (a.c.fuse_sharpen) {
       if (a.c.use_sharpen && a.c.use_dehalo) f *= sharpen_fact(a, psd, tb.wsh) * dehalo_fact(a, psd, tb.wdh);
       else if (a.c.use_sharpen) f *= sharpen_fact(a, psd, tb.wsh);
@@ -1394,11 +1411,13 @@ __device__ __forceinline__ void filter_inverse_group_cta(const InverseArgs& a, c
   __syncthreads();
   // 2. the separate sharpen/dehalo pass (src/code_impl/Sharpen.cpp:13-63),
   //    its grid fraction from each tile's filtered DC (published by the
-  //    filter stage); per bin pair, the pair's tables loaded once for all frames
+  //    filter stage); whole rounds of bin pairs with the pair's tables loaded
+  //    once for all frames, then the remaining pairs as (pair, frame) items
+  //    spread over every thread (as the filter stage does)
   if (a.c.do_sharpen) {
-    for (int p = t; p < PAIRS; p += NT) {
-      const int bin = 2 * p;
-      BinTab tb0{make_float2(0.f, 0.f), 0.f, 0.f}, tb1 = tb0;
+    auto tabs = [&](int bin, BinTab& tb0, BinTab& tb1) {
+      tb0 = BinTab{make_float2(0.f, 0.f), 0.f, 0.f};
+      tb1 = tb0;
       if (a.c.degrid != 0.f) {
         const float4 g = __ldg(reinterpret_cast<const float4*>(a.t.grid + bin));
         tb0.grid = make_float2(g.x, g.y);
@@ -1412,13 +1431,24 @@ __device__ __forceinline__ void filter_inverse_group_cta(const InverseArgs& a, c
         tb0.wdh = __ldg(a.t.wdehalo + bin);
         tb1.wdh = __ldg(a.t.wdehalo + bin + 1);
       }
-      for (int j = 0; j < count; j++) {
-        float4* q = reinterpret_cast<float4*>(S + j * BINS + bin);
-        const float4 v = *q;
-        const float2 v0 = sharpen_bin(a, make_float2(v.x, v.y), tb0, gsh[j]);
-        const float2 v1 = sharpen_bin(a, make_float2(v.z, v.w), tb1, gsh[j]);
-        *q = make_float4(v0.x, v0.y, v1.x, v1.y);
-      }
+    };
+    auto one = [&](int bin, int j, const BinTab& tb0, const BinTab& tb1) {
+      float4* q = reinterpret_cast<float4*>(S + j * BINS + bin);
+      const float4 v = *q;
+      const float2 v0 = sharpen_bin(a, make_float2(v.x, v.y), tb0, gsh[j]);
+      const float2 v1 = sharpen_bin(a, make_float2(v.z, v.w), tb1, gsh[j]);
+      *q = make_float4(v0.x, v0.y, v1.x, v1.y);
+    };
+    for (int p = t; p < FULL; p += NT) {
+      BinTab tb0, tb1;
+      tabs(2 * p, tb0, tb1);
+      for (int j = 0; j < count; j++) one(2 * p, j, tb0, tb1);
+    }
+    for (int i = t; i < (PAIRS - FULL) * count; i += NT) {
+      const int q = i / count, j = i - q * count;
+      BinTab tb0, tb1;
+      tabs(2 * (FULL + q), tb0, tb1);
+      one(2 * (FULL + q), j, tb0, tb1);
     }
     __syncthreads();
   }
