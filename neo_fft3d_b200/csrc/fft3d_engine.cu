@@ -1117,12 +1117,14 @@ int run_group(fft3d_plane* P, const fft3d::Deferred& d, cudaStream_t st) {
        "plane copy");
   std::vector<char> ola_done(d.ola.size(), 0);  // overlap-adds done by a run's launch
   for (size_t i = 0; P->group_split == 2 && i < d.inv.size();) {
-    // One launch per run of up to kGroupTile consecutive frames of one mode,
+    // One launch per run of up to group_run_frames consecutive frames of one mode,
     // one CTA per block: each window spectrum (and a Kalman state) is read
     // once for the run and every filtered tile stays in shared memory.
     const int mode = d.inv[i].mode;
     size_t e = i + 1;
-    while (e < d.inv.size() && d.inv[e].mode == mode && (int)(e - i) < fft3d::kGroupTile) e++;
+    while (e < d.inv.size() && d.inv[e].mode == mode &&
+           (int)(e - i) < fft3d::group_run_frames(P->g.bw, P->g.bh))
+      e++;
     const int n = (int)(e - i);
     fft3d::TemporalSet ts{};
     ts.count = n;

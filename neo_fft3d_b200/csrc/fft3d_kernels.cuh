@@ -143,6 +143,15 @@ struct FilterFrameSet {
 // the spectrum of frame n0 - 2 + s (null where no window of the run reaches),
 // tdom[j] receives frame n0 + j's time-domain blocks.
 constexpr int kGroupTile = 8;
+// Frames of one run for bw x bh blocks: up to kGroupTile, fewer where the
+// run's spectrum tiles (bh x (bw/2+1) complex per frame) would keep fewer
+// than 4 CTAs resident per SM (48 x 48 blocks: 5 frames, 4 CTAs instead of
+// 2 with 8 frames).
+__host__ __device__ constexpr int group_run_frames(int bw, int bh) {
+  return ((228 * 1024 / 4 - 1024 - 2 * kGroupTile * 4) / (bh * (bw / 2 + 1) * 8)) < kGroupTile
+             ? ((228 * 1024 / 4 - 1024 - 2 * kGroupTile * 4) / (bh * (bw / 2 + 1) * 8))
+             : kGroupTile;
+}
 struct TemporalSet {
   const float2* spec[kGroupTile + 4];
   float* tdom[kGroupTile];

@@ -1516,7 +1516,8 @@ __device__ __forceinline__ void filter_inverse_group_cta(const InverseArgs& a, c
 }
 
 template <int BW, int BH, int MODE>
-__global__ void __launch_bounds__(kWarps * 32, ctas_for(FFT3D_GROUP_CTAS, group_smem_bytes<BW, BH>(kGroupTile)))
+__global__ void __launch_bounds__(kWarps * 32,
+                                  ctas_for(FFT3D_GROUP_CTAS, group_smem_bytes<BW, BH>(group_run_frames(BW, BH))))
     k_filter_inverse_group(InverseArgs a,
                                                                      const __grid_constant__ TemporalSet ts,
                                                                      const __grid_constant__ OlaFuse of) {
@@ -1890,7 +1891,7 @@ cudaError_t inv_group_mode(const InverseArgs& a, const TemporalSet& ts, const Ol
 
 template <int BW, int BH>
 cudaError_t inv_group(const InverseArgs& a, const TemporalSet& ts, int mode, cudaStream_t s, const OlaFuse* ofp) {
-  if (ts.count < 1 || ts.count > kGroupTile) return cudaErrorInvalidValue;
+  if (ts.count < 1 || ts.count > group_run_frames(BW, BH)) return cudaErrorInvalidValue;
   OlaFuse of{};
   if (ofp) {
     of = *ofp;
