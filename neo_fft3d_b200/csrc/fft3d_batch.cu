@@ -579,7 +579,8 @@ int fft3d_batch_step(fft3d_batch* b, int count, fft3d_plane* const* planes, cons
   for (size_t i = 0; i < d.inv.size();) {
     size_t e = i + 1;
     while (e < d.inv.size() && planes[d.inv[e].plane] == planes[d.inv[i].plane] && d.inv[e].mode == d.inv[i].mode &&
-           d.inv[e].plane == d.inv[e - 1].plane + 1 && (int)(e - i) < fft3d::kGroupTile)
+           d.inv[e].plane == d.inv[e - 1].plane + 1 &&
+           (int)(e - i) < fft3d::group_run_frames(d.inv[i].a.g.bw, d.inv[i].a.g.bh))
       e++;
     if (e - i >= 2) {
       Deferred::Run run{};

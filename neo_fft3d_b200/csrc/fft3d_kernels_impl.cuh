@@ -1530,12 +1530,13 @@ __global__ void __launch_bounds__(kWarps * 32,
 // after every store) and they cost no registers.
 template <int BW, int BH, int MODE>
 __global__ void __launch_bounds__(kWarps * 32,
-                                  ctas_for(FFT3D_GROUP_CTAS, group_smem_bytes<BW, BH>(kGroupTile) + (int)sizeof(GroupRun)))
+                                  ctas_for(FFT3D_GROUP_CTAS,
+                                           group_smem_bytes<BW, BH>(group_run_frames(BW, BH)) + (int)sizeof(GroupRun)))
     k_filter_inverse_group_batch(const GroupRun* __restrict__ runs,
                                                                            const int2* __restrict__ items,
                                                                            int nitems) {
   extern __shared__ float2 smem2[];
-  GroupRun* sr = reinterpret_cast<GroupRun*>(smem2 + kGroupTile + kGroupTile * BH * (BW / 2 + 1));
+  GroupRun* sr = reinterpret_cast<GroupRun*>(smem2 + kGroupTile + group_run_frames(BW, BH) * BH * (BW / 2 + 1));
   static_assert(sizeof(GroupRun) % 4 == 0, "word copy");
   for (int i = blockIdx.x; i < nitems; i += gridDim.x) {
     const int2 it = items[i];
@@ -1741,7 +1742,7 @@ int occupancy_of(int which, int mode_or_bytes) {
   if (which == 0) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_forward_batch<BW, BH, uint8_t>, kWarps * 32, smem);
   } else if (which == 3) {
-    const int gsmem = group_smem_bytes<BW, BH>(kGroupTile) + (int)sizeof(GroupRun);
+    const int gsmem = group_smem_bytes<BW, BH>(group_run_frames(BW, BH)) + (int)sizeof(GroupRun);
     fft3d::smem_attr(k_filter_inverse_group_batch<BW, BH, 5>, gsmem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_filter_inverse_group_batch<BW, BH, 5>, kWarps * 32, gsmem);
   } else {
@@ -1913,7 +1914,7 @@ cudaError_t inv_group(const InverseArgs& a, const TemporalSet& ts, int mode, cud
 
 template <int BW, int BH, int MODE>
 cudaError_t inv_group_batch_mode(const BatchLaunch& l, cudaStream_t s) {
-  const int smem = group_smem_bytes<BW, BH>(kGroupTile) + (int)sizeof(GroupRun);
+  const int smem = group_smem_bytes<BW, BH>(group_run_frames(BW, BH)) + (int)sizeof(GroupRun);
   cudaError_t e = fft3d::smem_attr(k_filter_inverse_group_batch<BW, BH, MODE>, smem);
   if (e != cudaSuccess) return e;
   k_filter_inverse_group_batch<BW, BH, MODE><<<l.grid, kWarps * 32, smem, s>>>(static_cast<const GroupRun*>(l.args),
