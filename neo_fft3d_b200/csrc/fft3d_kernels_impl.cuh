@@ -58,6 +58,36 @@ __device__ __forceinline__ int field_row(int k, int H, int interlaced) {
   return k < half ? 2 * k : H - 1 - 2 * (k - half);
 }
 
+// The hardware's approximate reciprocal and reciprocal square root (PTX
+// rcp.approx / rsqrt.approx, the instructions __fdividef and rsqrtf stand on).
+// Every caller's argument is a normal float (a power spectrum plus 1e-15,
+// a noise power of at least 1e-15, a ratio clamped to >= 1e-30), where the
+// .ftz forms give the same result without the handling of denormal
+// arguments that the plain forms carry.
+__device__ __forceinline__ float rcp_nrm(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rsqrt_nrm(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// n / d for 0 <= n < 2^24, d > 0 and a quotient below 2^20 (pixel and block
+// coordinates over a block step or a row length), exact: the estimate
+// n * (1/d) is within (n / d) * 2^-21 < 0.5 of n / d (reciprocal <= 2 ulp,
+// one rounding), so truncating it and correcting by one step either way gives
+// the integer quotient, in a few instructions instead of an integer division
+// by a runtime value.
+__device__ __forceinline__ int div_small(int n, int d) {
+  int q = __float2int_rz(__int2float_rn(n) * rcp_nrm(__int2float_rn(d)));
+  const int r = n - q * d;
+  q += (r >= d) - (r < 0);
+  return q;
+}
+
 template <typename T>
 __device__ __forceinline__ float load_sample(const T* p) { return (float)p[0]; }
 template <>
@@ -138,7 +168,7 @@ template <typename T, class Win>
 __device__ __forceinline__ const T* fwd_row_src(const ForwardArgs& a, const Win& win, int blk, int y, int* x0,
                                                 int* row = nullptr) {
   const Geom& g = a.g;
-  const int by = blk / g.nox, bx = blk - by * g.nox;
+  const int by = div_small(blk, g.nox), bx = blk - by * g.nox;
   const int k = reflect101(by * g.sy + y - g.sy, g.H);
   *x0 = bx * g.sx - g.sx;
   const int r = field_row(k, g.H, g.interlaced);
@@ -461,35 +491,6 @@ __device__ __forceinline__ BinTab bin_tab(const InverseArgs& a, int bin) {
   if (sh && a.c.use_sharpen) t.wsh = __ldg(a.t.wsharpen + bin);
   if (sh && a.c.use_dehalo) t.wdh = __ldg(a.t.wdehalo + bin);
   return t;
-}
-
-// The hardware's approximate reciprocal and reciprocal square root (PTX
-// rcp.approx / rsqrt.approx, the instructions __fdividef and rsqrtf stand on).
-// Every caller's argument is a normal float (a power spectrum plus 1e-15,
-// a noise power of at least 1e-15, a ratio clamped to >= 1e-30), where the
-// .ftz forms give the same result without the handling of denormal
-// arguments that the plain forms carry.
-__device__ __forceinline__ float rcp_nrm(float x) {
-  float y;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-__device__ __forceinline__ float rsqrt_nrm(float x) {
-  float y;
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-
-// n / d for 0 <= n < 2^16 and 0 < d < 2^16 (pixel coordinates over a block
-// step), exact: the float estimate n * (1/d) is within 0.05 of n / d for these
-// ranges, so truncating it and correcting by one step either way gives the
-// integer quotient, in a few instructions instead of an integer division by
-// a runtime value.
-__device__ __forceinline__ int div_small(int n, int d) {
-  int q = __float2int_rz(__int2float_rn(n) * rcp_nrm(__int2float_rn(d)));
-  const int r = n - q * d;
-  q += (r >= d) - (r < 0);
-  return q;
 }
 
 // |c|^2 + 1e-15 of a bin (the reference's psd, src/code_impl/Apply.cpp:27-31)
@@ -1416,7 +1417,7 @@ __device__ __forceinline__ void filter_inverse_group_cta(const InverseArgs& a, c
       group_filter_pair<MODE>(a, ts, off, 2 * p, count, gfs, gsh, gs0, S + 2 * p, BINS);
   } else {
     for (int i = t; i < (PAIRS - FULL) * count; i += NT) {
-      const int q = i / count, j = i - q * count, p = FULL + q;
+      const int q = div_small(i, count), j = i - q * count, p = FULL + q;
       group_filter_one<MODE>(a, ts, off, 2 * p, j, gfs, gsh, gs0, S + j * BINS + 2 * p);
     }
   }
@@ -1457,7 +1458,7 @@ __device__ __forceinline__ void filter_inverse_group_cta(const InverseArgs& a, c
       for (int j = 0; j < count; j++) one(2 * p, j, tb0, tb1);
     }
     for (int i = t; i < (PAIRS - FULL) * count; i += NT) {
-      const int q = i / count, j = i - q * count;
+      const int q = div_small(i, count), j = i - q * count;
       BinTab tb0, tb1;
       tabs(2 * (FULL + q), tb0, tb1);
       one(2 * (FULL + q), j, tb0, tb1);
