@@ -270,3 +270,38 @@ def test_reset_waits_for_queued_work(gpu, grouped):
     for o in outs[1:]:
         assert torch.equal(outs[0], o)
     e.close()
+
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("bw,runs", [(32, 1), (48, 2)])
+def test_frame_group_runs_capped_by_block_size(gpu, bw, runs):
+    """A group of 8 interior frames is one filter/inverse run for 32x32 blocks
+    and two runs (5 + 3 frames) for 48x48 blocks, whose 8-frame tiles would
+    leave only 2 CTAs per SM; the output still equals one frame per call."""
+    import torch
+    clip = dict(width=176, height=144, bits=8, seed=83)
+    filt = dict(sigma=2.5, bt=3, bw=bw, bh=bw, ow=16, oh=16)
+    planes, dev = _clip(torch, clip)
+    ref = _per_frame(torch, planes[:1], dev[:1], clip, filt)[0]
+    e = _engines(planes[:1], clip, filt)[0]
+    a = dev[0]
+    o = torch.full_like(a, 1)  # a value no filtered sample takes: unwritten pixels show
+    st = a.shape[2]
+
+    def group(n0, k):
+        e.filter_frames_device(n0, [_ptr(a, n) for n in range(n0 - 2, n0 + k + 2)], [st] * (k + 4),
+                               [_ptr(o, n) for n in range(n0, n0 + k)], [st] * k, 0)
+
+    group(0, 6)
+    e.timing()
+    e.set_timing(True)
+    group(6, 8)  # frames 6..13: interior (btcur = bt), one mode
+    torch.cuda.synchronize()
+    t = e.timing()
+    e.set_timing(False)
+    assert t["filter_inverse"][0] == runs
+    group(14, F - 14)
+    torch.cuda.synchronize()
+    assert np.array_equal(o.cpu().numpy(), ref)
+    e.close()
